@@ -1,0 +1,148 @@
+// trtc_compact.cuh -- single-pass stable stream compaction and partition.
+//
+// Replaces the reference's compaction shape (internal/general_copy_if.cpp:26-64 and the
+// partition scans of partition.cpp:29-125): a u32 flag scan through general_scan, a
+// blocking copy of the count to the host, then a scatter kernel.  Here one kernel computes
+// the flags from the tile it holds in registers, ranks the selected elements with warp
+// ballots, finds the tile's output offset by decoupled look-back over selected counts and
+// writes the selected elements (and, for partitions, the rejected ones at
+// index - selected_before).  Inputs are read before a tile publishes anything, so the
+// in-place forms (Remove, Remove_If, Unique, ...) need no copy of the input.
+#pragma once
+#include "trtc_scan.cuh"
+
+namespace trtc {
+
+enum CompactMode : int {
+    CM_PRED = 0,             // pred(in[i])                       copy_if / partition
+    CM_PRED_STENCIL = 1,     // pred(stencil[i])                  copy_if_stencil / partition_stencil
+    CM_NOT_EQUAL = 2,        // in[i] != value                    remove / remove_copy
+    CM_NOT_PRED = 3,         // !pred(in[i])                      remove_if / remove_copy_if
+    CM_NOT_PRED_STENCIL = 4, // !pred(stencil[i])                 remove_if_stencil
+    CM_UNIQUE = 5,           // i == 0 || in[i] != in[i-1]        unique (default)
+    CM_UNIQUE_PRED = 6,      // i == 0 || !pred(in[i], in[i-1])   unique with binary_pred
+    CM_TAIL = 7,             // i == n-1 || !pred(in[i], in[i+1]) reduce_by_key segment tails
+};
+
+template <int MODE, bool PARTITION, bool TWO, class InV, class StV, class Pred, class ValT, class OutV, class FalseV,
+          class In2V, class Out2V, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pred pred, ValT value, OutV out,
+                                                        FalseV out_false, In2V in2, Out2V out2, size_t n,
+                                                        LookbackState st) {
+    typedef typename remove_cvref<typename InV::value_t>::type E;
+    typedef typename remove_cvref<decltype(in2[0])>::type E2;
+    constexpr int WARPS = BLOCK / 32;
+    constexpr int TILE = BLOCK * ITEMS;
+    __shared__ uint32_t s_slot[2];
+    __shared__ uint32_t s_wcnt[WARPS];
+    __shared__ unsigned long long s_pre;
+
+    const size_t tile = claim_tile(st, s_slot);
+    const size_t tile_base = tile * TILE;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const size_t wbase = tile_base + (size_t)warp * 32 * ITEMS;
+    const uint32_t ltm = lanemask_lt();
+
+    E v[ITEMS];
+    E2 v2[TWO ? ITEMS : 1];
+    bool f[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const size_t idx = wbase + (size_t)i * 32 + lane;
+        const bool ok = idx < n;
+        v[i] = ok ? (E)in[idx] : E();
+        if constexpr (TWO) v2[i] = ok ? (E2)in2[idx] : E2();
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const size_t idx = wbase + (size_t)i * 32 + lane;
+        const bool ok = idx < n;
+        bool sel = false;
+        if constexpr (MODE == CM_PRED) sel = ok && (bool)pred(v[i]);
+        else if constexpr (MODE == CM_PRED_STENCIL) sel = ok && (bool)pred(stencil[idx < n ? idx : 0]);
+        else if constexpr (MODE == CM_NOT_EQUAL) sel = ok && !(v[i] == value);
+        else if constexpr (MODE == CM_NOT_PRED) sel = ok && !(bool)pred(v[i]);
+        else if constexpr (MODE == CM_NOT_PRED_STENCIL) sel = ok && !(bool)pred(stencil[idx < n ? idx : 0]);
+        else if constexpr (MODE == CM_UNIQUE || MODE == CM_UNIQUE_PRED) {
+            E prev = shfl_up_any(v[i], 1);
+            const E last = i > 0 ? shfl_any(v[i > 0 ? i - 1 : 0], 31) : E();
+            if (lane == 0) prev = (i > 0) ? last : ((ok && idx > 0) ? (E)in[idx - 1] : E());
+            if constexpr (MODE == CM_UNIQUE) sel = ok && (idx == 0 || v[i] != prev);
+            else sel = ok && (idx == 0 || !(bool)pred(v[i], prev));
+        } else if constexpr (MODE == CM_TAIL) {
+            E next = shfl_down_any(v[i], 1);
+            const E first = i + 1 < ITEMS ? shfl_any(v[i + 1 < ITEMS ? i + 1 : i], 0) : E();
+            if (lane == 31) next = (i + 1 < ITEMS) ? first : ((idx + 1 < n) ? (E)in[idx + 1] : E());
+            sel = ok && (idx + 1 == n || !(bool)pred(v[i], next));
+        }
+        f[i] = sel;
+    }
+    // warp ranks
+    uint32_t rank[ITEMS];
+    uint32_t wc = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const uint32_t b = __ballot_sync(0xffffffffu, f[i]);
+        rank[i] = wc + (uint32_t)__popc(b & ltm);
+        wc += (uint32_t)__popc(b);
+    }
+    if (lane == 0) s_wcnt[warp] = wc;
+    __syncthreads();
+
+    if (warp == 0) {
+        unsigned long long agg = 0;
+        if (lane < (uint32_t)WARPS) agg = s_wcnt[lane];
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) agg += __shfl_down_sync(0xffffffffu, agg, d);
+        agg = __shfl_sync(0xffffffffu, agg, 0);
+        unsigned long long pre = 0;
+        Plus plus;
+        if (tile > 0) {
+            if (lane == 0) publish<unsigned long long>(st, tile, agg, false, false);
+            bool dummy;
+            pre = lookback_prefix<unsigned long long, Plus, false>(st, tile, plus, dummy).v;
+        }
+        if (lane == 0) {
+            publish<unsigned long long>(st, tile, pre + agg, true, false);
+            if (tile_base + TILE >= n && st.result) *reinterpret_cast<unsigned long long*>(st.result) = pre + agg;
+            s_pre = pre;
+        }
+    }
+    __syncthreads();
+
+    unsigned long long base = s_pre;
+    for (uint32_t w = 0; w < warp; w++) base += s_wcnt[w];
+    const size_t out_n = out.size();
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const size_t idx = wbase + (size_t)i * 32 + lane;
+        if (idx >= n) continue;
+        const unsigned long long before = base + rank[i];  // selected elements before idx
+        if (f[i]) {
+            if (before < out_n) {
+                out[before] = v[i];
+                if constexpr (TWO) {
+                    if (before < (unsigned long long)out2.size()) out2[before] = v2[i];
+                }
+            }
+        } else {
+            if constexpr (PARTITION) {
+                const unsigned long long fp = idx - before;
+                if (fp < (unsigned long long)out_false.size()) out_false[fp] = v[i];
+            }
+        }
+    }
+}
+
+// Partition in place: rejected elements were compacted into a temp buffer; move them
+// behind the selected ones once the count is known on the device.
+template <class E>
+__global__ void partition_tail_kernel(const E* __restrict__ tmp, E* __restrict__ out, size_t n,
+                                      const unsigned long long* count) {
+    const unsigned long long c = *count;
+    const size_t nf = n - (size_t)c;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += (size_t)gridDim.x * blockDim.x)
+        out[c + i] = tmp[i];
+}
+
+}  // namespace trtc

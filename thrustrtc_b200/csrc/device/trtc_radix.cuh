@@ -1,0 +1,453 @@
+// trtc_radix.cuh -- onesweep LSD radix sort (8-bit digits) for the built-in key types.
+//
+// Replaces the reference's 1-bit-per-pass split sort (internal/radix_sort.cpp:165-553),
+// producing the identical stable order:
+//   * hist kernel: one read of the keys builds the 256-bin histogram of every digit of the
+//     ordered key code (RadixKey<K>::ordered), flags NaNs, and clears the first look-back
+//     status array;
+//   * plan kernel: marks digits whose histogram has a bucket holding every key as no-ops
+//     (the reference's varying-bit mask, internal/radix_sort.cpp:11-45, at digit granularity),
+//     scans the histograms into bucket bases and picks the ping-pong buffer of every pass so
+//     the result lands in the caller's buffer without a host round trip;
+//   * min-tree + count kernels (float/double, only when a NaN is present): the reference
+//     offsets keys by keys[TRTC_Min_Element], whose 256-wide tree (extrema.cpp:5-13 over
+//     internal/general_reduce.cpp:55-95) can select a non-minimum when NaNs sit in left slots;
+//     the sorted order is then a rotation, applied by the last digit pass's scatter;
+//   * one pass kernel per digit: a CTA takes tiles in launch order from an atomic counter,
+//     ranks its keys with warp multisplit (__match_any_sync), publishes per-digit counts,
+//     looks back across earlier tiles for its global offsets (decoupled look-back with
+//     release/acquire flags and bounded spins), stages the tile in shared memory in digit
+//     order and writes it out in bucket runs.
+#pragma once
+#include "trtc_prelude.cuh"
+
+namespace trtc {
+
+struct SortPlan {
+    uint32_t active_mask;      // bit p: digit pass p moves data
+    uint32_t num_active;
+    int32_t ordinal[8];        // running index of active pass p (selects the status array)
+    uint32_t src_sel[8];       // buffer set a pass reads: 0 caller, 1 temp A, 2 temp B
+    uint32_t dst_sel[8];
+    int32_t last_pass;         // last active pass (applies the rotation)
+    uint32_t copy_back;        // one active pass only: result sits in temp A
+    uint32_t base[8][256];     // exclusive bucket starts of every pass
+};
+
+// Per-call control block; the host zeroes it (one memset) before every sort.
+struct SortCtrl {
+    uint32_t hist[8][256];
+    uint32_t tile_ctr[8];
+    uint32_t nan_flag;
+    uint32_t err;
+    unsigned long long rot_count;   // keys ordered strictly below the selected minimum
+    SortPlan plan;
+};
+
+struct SortBufs {
+    void* keys[3];
+    void* vals[3];
+    uint32_t* err;   // host-visible error word
+};
+
+template <class S> struct StatusBits;
+template <> struct StatusBits<uint32_t> {
+    static constexpr int SHIFT = 30;
+    static constexpr uint32_t MASK = 0x3FFFFFFFu;
+};
+template <> struct StatusBits<unsigned long long> {
+    static constexpr int SHIFT = 62;
+    static constexpr unsigned long long MASK = 0x3FFFFFFFFFFFFFFFull;
+};
+
+template <class K, bool DESC>
+TRTC_FORCEINLINE uint32_t radix_digit(typename RadixKey<K>::B k, int shift) {
+    typename RadixKey<K>::U u = RadixKey<K>::ordered(k);
+    if (DESC) u = ~u;
+    return (uint32_t)(u >> shift) & 0xFFu;
+}
+
+// inclusive scan over the 256 threads of a (sub)block; threads >= 256 must also call it
+template <int BLOCK>
+__device__ inline uint32_t block_excl_scan_256(uint32_t v, uint32_t* s_wsum) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (t < 256 && lane == 31) s_wsum[w] = x;
+    __syncthreads();
+    uint32_t pre = 0;
+    if (t < 256)
+        for (int i = 0; i < w; i++) pre += s_wsum[i];
+    __syncthreads();
+    return pre + x - v;
+}
+
+// ------------------------------------------------------------------ histogram
+template <class K, bool DESC, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) radix_hist_kernel(const typename RadixKey<K>::B* __restrict__ keys, size_t n,
+                                                           SortCtrl* ctrl, uint4* status0, size_t status_vec4) {
+    typedef RadixKey<K> RK;
+    typedef typename RK::B KB;
+    constexpr int D = RK::DIGITS;
+    __shared__ uint32_t sh[D][256];
+    __shared__ uint32_t s_nan;
+    for (int i = threadIdx.x; i < D * 256; i += BLOCK) (&sh[0][0])[i] = 0;
+    if (threadIdx.x == 0) s_nan = 0;
+    __syncthreads();
+
+    // clear the first look-back status array (the pass kernels clear the next one)
+    for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < status_vec4; i += (size_t)gridDim.x * BLOCK)
+        status0[i] = make_uint4(0u, 0u, 0u, 0u);
+
+    const uint32_t lane = threadIdx.x & 31u;
+    bool any_nan = false;
+    auto count_key = [&](KB k, bool valid) {
+        const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
+        if (!vmask) return;
+        const int src = __ffs(vmask) - 1;
+        if (valid) any_nan |= RK::is_nan(k);
+        typename RK::U u = RK::ordered(k);
+        if (DESC) u = ~u;
+#pragma unroll
+        for (int p = 0; p < D; p++) {
+            const uint32_t d = (uint32_t)(u >> (8 * p)) & 0xFFu;
+            const uint32_t first = __shfl_sync(0xffffffffu, d, src);
+            if (__all_sync(0xffffffffu, !valid || d == first)) {
+                if ((int)lane == src) atomicAdd(&sh[p][first], (uint32_t)__popc(vmask));
+            } else if (valid) {
+                atomicAdd(&sh[p][d], 1u);
+            }
+        }
+    };
+
+    constexpr int VEC = 16 / (int)sizeof(KB);
+    const size_t nvec = ((((size_t)keys) & 15) == 0) ? n / VEC : 0;
+    const size_t warps_total = (size_t)gridDim.x * (BLOCK / 32);
+    const size_t gwarp = (size_t)blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5);
+    // vectorised body: each lane takes one 16-byte vector per round
+    for (size_t base = gwarp * 32; base < nvec; base += warps_total * 32) {
+        const size_t vi = base + lane;
+        const bool valid = vi < nvec;
+        union { uint4 q; KB k[VEC]; } u;
+        if (valid) u.q = reinterpret_cast<const uint4*>(keys)[vi];
+#pragma unroll
+        for (int e = 0; e < VEC; e++) count_key(valid ? u.k[e] : KB(0), valid);
+    }
+    // scalar tail (and unaligned inputs)
+    for (size_t base = nvec * VEC + gwarp * 32; base < n; base += warps_total * 32) {
+        const size_t i = base + lane;
+        const bool valid = i < n;
+        count_key(valid ? keys[i] : KB(0), valid);
+    }
+    if (any_nan) s_nan = 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < D * 256; i += BLOCK) {
+        const uint32_t c = (&sh[0][0])[i];
+        if (c) atomicAdd(&ctrl->hist[0][0] + i, c);
+    }
+    if (threadIdx.x == 0 && s_nan) atomicOr(&ctrl->nan_flag, 1u);
+}
+
+// ------------------------------------------------------------------ plan (1 block of 256)
+template <int D>
+__global__ void __launch_bounds__(256) radix_plan_kernel(SortCtrl* ctrl, size_t n) {
+    __shared__ uint32_t s_wsum[8];
+    __shared__ uint32_t s_active[8];
+    const int t = threadIdx.x;
+    for (int p = 0; p < D; p++) {
+        const uint32_t c = ctrl->hist[p][t];
+        const int full = __syncthreads_or(c == (uint32_t)n);
+        const uint32_t ex = block_excl_scan_256<256>(c, s_wsum);
+        ctrl->plan.base[p][t] = ex;
+        if (t == 0) s_active[p] = full ? 0u : 1u;
+    }
+    __syncthreads();
+    if (t == 0) {
+        SortPlan& pl = ctrl->plan;
+        uint32_t mask = 0;
+        for (int p = 0; p < D; p++) mask |= s_active[p] << p;
+        const int a = __popc(mask);
+        pl.active_mask = mask;
+        pl.num_active = (uint32_t)a;
+        pl.copy_back = (a == 1) ? 1u : 0u;
+        pl.last_pass = -1;
+        int j = 0;
+        uint32_t cur = 0;
+        for (int p = 0; p < 8; p++) {
+            pl.ordinal[p] = 0; pl.src_sel[p] = 0; pl.dst_sel[p] = 0;
+            if (p >= D || !((mask >> p) & 1u)) continue;
+            uint32_t dst;
+            if (a == 1) dst = 1;
+            else if ((a & 1) == 0) dst = (j & 1) ? 0u : 1u;
+            else if (j == 0) dst = 1;
+            else if (j == 1) dst = 2;
+            else if (j == 2) dst = 0;
+            else dst = (j & 1) ? 1u : 0u;
+            pl.ordinal[p] = j;
+            pl.src_sel[p] = cur;
+            pl.dst_sel[p] = dst;
+            pl.last_pass = p;
+            cur = dst;
+            j++;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ Min_Element tree
+// Exact replica of the reference's index reduction order: consecutive blocks of 256, inside
+// a block the strided tree s = 128..1 with "if (tid < s && i + s < n) h[tid] = op(h[tid],
+// h[tid+s])", op(i1, i2) = v[i2] < v[i1] ? i2 : i1.  One warp handles one 256-block: lane l
+// holds slots l, l+32, ..., l+224.  FIRST: read keys; otherwise read a previous round.
+template <class K, bool FIRST, bool NAN_GATE>
+__global__ void __launch_bounds__(256) min_tree_kernel(const typename RadixKey<K>::B* __restrict__ keys,
+                                                        const K* __restrict__ in_v,
+                                                        const unsigned long long* __restrict__ in_i, size_t m,
+                                                        K* __restrict__ out_v, unsigned long long* __restrict__ out_i,
+                                                        const SortCtrl* ctrl) {
+    if (NAN_GATE && ctrl->nan_flag == 0) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const size_t nb = (m + 255) / 256;
+    const size_t warps_total = (size_t)gridDim.x * (blockDim.x / 32);
+    for (size_t b = (size_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); b < nb; b += warps_total) {
+        const size_t base = b * 256;
+        const uint32_t L = (uint32_t)((m - base) < 256 ? (m - base) : 256);
+        K v[8];
+        unsigned long long ix[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t t = lane + 32u * k;
+            if (t < L) {
+                if (FIRST) { v[k] = RadixKey<K>::value(keys[base + t]); ix[k] = base + t; }
+                else { v[k] = in_v[base + t]; ix[k] = in_i[base + t]; }
+            } else {
+                v[k] = K(); ix[k] = 0;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (lane + 32u * k + 128u < L && v[k + 4] < v[k]) { v[k] = v[k + 4]; ix[k] = ix[k + 4]; }
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+            if (lane + 32u * k + 64u < L && v[k + 2] < v[k]) { v[k] = v[k + 2]; ix[k] = ix[k + 2]; }
+        if (lane + 32u < L && v[1] < v[0]) { v[0] = v[1]; ix[0] = ix[1]; }
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const K ov = shfl_down_any(v[0], s);
+            const unsigned long long oi = __shfl_down_sync(0xffffffffu, ix[0], s);
+            if (lane < (uint32_t)s && lane + s < L && ov < v[0]) { v[0] = ov; ix[0] = oi; }
+        }
+        if (lane == 0) { out_v[b] = v[0]; out_i[b] = ix[0]; }
+    }
+}
+
+// number of keys whose ordered code is below the selected minimum's (NaN case only)
+template <class K, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) radix_count_below_kernel(const typename RadixKey<K>::B* __restrict__ keys, size_t n,
+                                                                  const unsigned long long* min_idx, SortCtrl* ctrl) {
+    if (ctrl->nan_flag == 0) return;
+    typedef RadixKey<K> RK;
+    const typename RK::U tm = RK::ordered(keys[*min_idx]);
+    unsigned long long c = 0;
+    for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK)
+        c += RK::ordered(keys[i]) < tm ? 1ull : 0ull;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(0xffffffffu, c, d);
+    if ((threadIdx.x & 31u) == 0 && c) atomicAdd(&ctrl->rot_count, c);
+}
+
+// ------------------------------------------------------------------ one digit pass
+// HAS_VALS: move a 4- or 8-byte payload with the keys.  vals_from_index: the payload of the
+// first active pass is the element index (used to sort a permutation for odd value sizes).
+template <class K, class V, bool HAS_VALS, bool DESC, int BLOCK, int ITEMS, class ST>
+__global__ void __launch_bounds__(BLOCK) radix_pass_kernel(SortBufs bufs, size_t n, SortCtrl* ctrl, int pass,
+                                                           ST* status0, ST* status1, int vals_from_index) {
+    static_assert(BLOCK >= 256, "one thread per digit is needed");
+    constexpr int TILE = BLOCK * ITEMS;
+    constexpr int WARPS = BLOCK / 32;
+    typedef StatusBits<ST> SB;
+    typedef typename RadixKey<K>::B KB;
+    const SortPlan& plan = ctrl->plan;
+    if (!((plan.active_mask >> pass) & 1u)) return;
+
+    extern __shared__ __align__(16) unsigned char smem[];
+    KB* s_keys = reinterpret_cast<KB*>(smem);
+    V* s_vals = reinterpret_cast<V*>(smem + sizeof(KB) * TILE);
+    uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem + sizeof(KB) * TILE + (HAS_VALS ? sizeof(V) * TILE : 0));
+    __shared__ uint32_t s_count[256], s_start[256], s_adj[256], s_wsum[8];
+    __shared__ uint32_t s_tile;
+
+    const int ord = plan.ordinal[pass];
+    ST* st = (ord & 1) ? status1 : status0;
+    ST* st_next = (ord & 1) ? status0 : status1;
+    // buffer selection with selects (a runtime index into the parameter array would copy
+    // it to local memory)
+    const uint32_t ss = plan.src_sel[pass], ds = plan.dst_sel[pass];
+    const KB* __restrict__ src_k =
+        reinterpret_cast<const KB*>(ss == 0 ? bufs.keys[0] : (ss == 1 ? bufs.keys[1] : bufs.keys[2]));
+    KB* __restrict__ dst_k = reinterpret_cast<KB*>(ds == 0 ? bufs.keys[0] : (ds == 1 ? bufs.keys[1] : bufs.keys[2]));
+    const V* __restrict__ src_v =
+        reinterpret_cast<const V*>(ss == 0 ? bufs.vals[0] : (ss == 1 ? bufs.vals[1] : bufs.vals[2]));
+    V* __restrict__ dst_v = reinterpret_cast<V*>(ds == 0 ? bufs.vals[0] : (ds == 1 ? bufs.vals[1] : bufs.vals[2]));
+    const int shift = pass * 8;
+    const bool index_payload = HAS_VALS && vals_from_index && ord == 0;
+    unsigned long long rot = 0;
+    if (pass == plan.last_pass && ctrl->rot_count) {
+        const unsigned long long k = ctrl->rot_count % n;
+        rot = DESC ? k : (k ? n - k : 0);
+    }
+
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ctrl->tile_ctr[ord], 1u);
+    for (int i = threadIdx.x; i < WARPS * 256; i += BLOCK) s_whist[i] = 0;
+    __syncthreads();
+    const size_t tile = s_tile;
+    for (int i = threadIdx.x; i < 256; i += BLOCK) st_next[tile * 256 + i] = 0;
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const size_t tile_base = tile * TILE;
+    const size_t wbase = tile_base + (size_t)warp * 32 * ITEMS;
+    const bool full = tile_base + TILE <= n;
+
+    KB keys[ITEMS];
+    V vals[HAS_VALS ? ITEMS : 1];
+    uint32_t rank[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const size_t idx = wbase + (size_t)i * 32 + lane;
+        if (full || idx < n) {
+            keys[i] = src_k[idx];
+            if (HAS_VALS) vals[i] = index_payload ? (V)idx : src_v[idx];
+        } else {
+            keys[i] = KB(0);
+            if (HAS_VALS) vals[i] = V();
+        }
+    }
+
+    // warp multisplit ranking: stable within the warp (items in order, lanes in order)
+    uint32_t* wh = s_whist + warp * 256;
+    const uint32_t ltm = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const size_t idx = wbase + (size_t)i * 32 + lane;
+        const uint32_t d = (full || idx < n) ? radix_digit<K, DESC>(keys[i], shift) : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t before = 0;
+        if (lane == leader && d < 256u) {
+            before = wh[d];
+            wh[d] = before + (uint32_t)__popc(peers);
+        }
+        before = __shfl_sync(0xffffffffu, before, leader);
+        rank[i] = before + (uint32_t)__popc(peers & ltm);
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // per-digit tile counts, warp prefixes, publication of the tile aggregate
+    uint32_t cnt = 0;
+    if (threadIdx.x < 256) {
+        const int d = threadIdx.x;
+        uint32_t sum = 0;
+#pragma unroll
+        for (int w = 0; w < WARPS; w++) {
+            const uint32_t c = s_whist[w * 256 + d];
+            s_whist[w * 256 + d] = sum;
+            sum += c;
+        }
+        cnt = sum;
+        s_count[d] = sum;
+        const ST flag = (ST)(tile == 0 ? 2u : 1u) << SB::SHIFT;
+        st_release(&st[tile * 256 + d], flag | (ST)sum);
+    }
+    const uint32_t start = block_excl_scan_256<BLOCK>(cnt, s_wsum);
+    if (threadIdx.x < 256) s_start[threadIdx.x] = start;
+    __syncthreads();
+
+    // stage the tile in digit order
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const size_t idx = wbase + (size_t)i * 32 + lane;
+        if (full || idx < n) {
+            const uint32_t d = radix_digit<K, DESC>(keys[i], shift);
+            const uint32_t pos = s_start[d] + wh[d] + rank[i];
+            s_keys[pos] = keys[i];
+            if (HAS_VALS) s_vals[pos] = vals[i];
+        }
+    }
+
+    // decoupled look-back, one thread per digit
+    if (threadIdx.x < 256) {
+        const int d = threadIdx.x;
+        ST excl = 0;
+        if (tile > 0) {
+            size_t j = tile - 1;
+            uint32_t spins = 0;
+            while (true) {
+                const ST s = ld_acquire(&st[j * 256 + d]);
+                const uint32_t f = (uint32_t)(s >> SB::SHIFT);
+                if (f == 0) {
+                    if (!spin_continue(spins, bufs.err)) { report_error(bufs.err, TRTC_ERR_LOOKBACK_TIMEOUT); break; }
+                    continue;
+                }
+                excl += s & SB::MASK;
+                if (f == 2 || j == 0) break;
+                --j;
+            }
+            st_release(&st[tile * 256 + d], ((ST)2u << SB::SHIFT) | (excl + (ST)s_count[d]));
+        }
+        s_adj[d] = plan.base[pass][d] + (uint32_t)excl - s_start[d];
+    }
+    __syncthreads();
+
+    // write out in bucket runs
+    const uint32_t tile_n = full ? (uint32_t)TILE : (uint32_t)(n - tile_base);
+    for (uint32_t k = threadIdx.x; k < tile_n; k += BLOCK) {
+        const KB key = s_keys[k];
+        const uint32_t d = radix_digit<K, DESC>(key, shift);
+        unsigned long long dst = (uint32_t)(s_adj[d] + k);
+        if (rot) { dst += rot; if (dst >= n) dst -= n; }
+        if (dst < n) {
+            dst_k[dst] = key;
+            if (HAS_VALS) dst_v[dst] = s_vals[k];
+        } else {
+            report_error(bufs.err, TRTC_ERR_BAD_PLAN);
+        }
+    }
+}
+
+// single active pass: the result sits in temp A and is copied back to the caller's buffers
+template <class K, class V, bool HAS_VALS>
+__global__ void radix_copyback_kernel(SortBufs bufs, size_t n, const SortCtrl* ctrl) {
+    if (!ctrl->plan.copy_back) return;
+    typedef typename RadixKey<K>::B KB;
+    const KB* sk = reinterpret_cast<const KB*>(bufs.keys[1]);
+    KB* dk = reinterpret_cast<KB*>(bufs.keys[0]);
+    const V* sv = reinterpret_cast<const V*>(bufs.vals[1]);
+    V* dv = reinterpret_cast<V*>(bufs.vals[0]);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        dk[i] = sk[i];
+        if (HAS_VALS) dv[i] = sv[i];
+    }
+}
+
+// payloads of other sizes: values[i] = values_orig[perm[i]] through a temp copy
+static __global__ void radix_gather_bytes_kernel(const unsigned char* __restrict__ vals, unsigned char* __restrict__ tmp,
+                                          const uint32_t* __restrict__ perm, size_t n, int esize, const SortCtrl* ctrl) {
+    if (ctrl->plan.num_active == 0) return;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t s = perm[i];
+        if (s >= n) continue;
+        for (int b = 0; b < esize; b++) tmp[i * esize + b] = vals[s * esize + b];
+    }
+}
+static __global__ void radix_copy_bytes_gated_kernel(const unsigned char* __restrict__ src, unsigned char* __restrict__ dst,
+                                              size_t nbytes, const SortCtrl* ctrl) {
+    if (ctrl->plan.num_active == 0) return;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nbytes; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+}  // namespace trtc

@@ -1,0 +1,605 @@
+// trtc_scan.cuh -- single-pass scans (decoupled look-back), segmented scans and reductions.
+//
+// Replaces the reference's 512-element block scan + recursive block-sum scan + add-back
+// (internal/general_scan.cpp:8-88), its segmented variant with an 'active' array
+// (internal/general_scan_by_key.cpp:8-143) and its 256-wide recursive tree reduction
+// (internal/general_reduce.cpp:30-95) with one pass over the data each.
+//
+// Tiles are claimed in launch order from an atomic counter, so a tile only ever waits for
+// tiles that are already running.  Every wait is bounded (TRTC_SPIN_LIMIT) and reports an
+// error instead of hanging.  Look-back flags are tagged with a per-call epoch so the flag
+// array never needs clearing between calls.  Operators need only be associative: all
+// combinations keep index order (older operand on the left), no identity element is used.
+#pragma once
+#include "trtc_prelude.cuh"
+#include "trtc_builtins.cuh"
+#include "trtc_abi.h"
+
+namespace trtc {
+
+
+// ---------------------------------------------------------------- loaders
+// A scan source: element i of the scanned sequence is get(fetch(i)) (a view read, optionally
+// followed by the unary op of a transform scan), converted to the scan's value type T.
+template <class InV, class T, class UOp, bool HAS_UOP>
+struct ScanSrc {
+    typedef typename remove_cvref<typename InV::value_t>::type E;
+    static constexpr bool CONTIG = ViewTraits<InV>::contiguous;
+    InV in;
+    UOp uop;
+    TRTC_FORCEINLINE T get(const E& raw) {
+        if constexpr (HAS_UOP) return (T)uop(raw);
+        else return (T)raw;
+    }
+    TRTC_FORCEINLINE E fetch(size_t i) { return in[i]; }
+};
+
+template <class E> struct VecWidth {
+    static constexpr int V = (sizeof(E) == 1 || sizeof(E) == 2 || sizeof(E) == 4 || sizeof(E) == 8 || sizeof(E) == 16)
+                                 ? (int)(16 / sizeof(E)) : 1;
+};
+
+template <class T> struct Opt { T v; bool h; };
+
+// a ⊕ b with optional operands (either may be absent)
+template <class T, class Op>
+TRTC_FORCEINLINE void opt_combine(T& a, bool& ah, const T& b, bool bh, Op& op) {
+    if (bh) { a = ah ? (T)op(a, b) : b; ah = true; }
+}
+
+// ---------------------------------------------------------------- look-back (warp 0)
+// Returns the ordered combination of all tiles before `tile` (their values being inclusive
+// prefixes or aggregates).  SEG: stop at the first tile holding a segment head as well, and
+// combine with the segmented operator (a head in the right operand discards the left).
+template <class T, class Op, bool SEG>
+__device__ inline Opt<T> lookback_prefix(const LookbackState& st, size_t tile, Op& op, bool& seg_flag_out) {
+    const uint32_t lane = lane_id();
+    const T* agg = reinterpret_cast<const T*>(st.agg);
+    const T* inc = reinterpret_cast<const T*>(st.incl);
+    T acc = T();
+    bool has = false, acc_head = false;
+    long long j0 = (long long)tile - 1;
+    while (j0 >= 0) {
+        const long long j = j0 - (long long)lane;
+        uint32_t state = 3;  // beyond tile 0: acts as a stop with no value
+        if (j >= 0) {
+            uint32_t spins = 0;
+            while (true) {
+                const uint32_t raw = ld_acquire(&st.flags[j]);
+                if (raw >= st.epoch4 + 1u && raw <= st.epoch4 + 2u) { state = raw - st.epoch4; break; }
+                if (!spin_continue(spins, st.err)) { report_error(st.err, TRTC_ERR_LOOKBACK_TIMEOUT); state = 2; break; }
+            }
+        }
+        T v = T();
+        bool hd = false;
+        if (j >= 0) {
+            v = (state == 2) ? inc[j] : agg[j];
+            if (SEG) hd = st.heads[j] != 0;
+        }
+        const uint32_t stop_mask = __ballot_sync(0xffffffffu, state >= 2u || (SEG && hd));
+        const int stop = stop_mask ? __ffs(stop_mask) - 1 : 31;
+        bool vh = (int)lane <= stop && j >= 0;
+        // ordered tree: lane l combines with lane l+d (older => left operand)
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const T o = shfl_down_any(v, d);
+            const int oh_i = __shfl_down_sync(0xffffffffu, (int)vh, d);
+            const int ohd = __shfl_down_sync(0xffffffffu, (int)hd, d);
+            const bool oh = oh_i && ((int)lane + d < 32);
+            if ((lane & (2 * d - 1)) == 0 && oh) {
+                if (SEG) {
+                    // o (older) ⊕ v (newer): a head in v keeps v
+                    if (!vh) { v = o; hd = ohd; }
+                    else if (!hd) { v = (T)op(o, v); hd = ohd; }
+                } else {
+                    v = vh ? (T)op(o, v) : o;
+                }
+                vh = true;
+            }
+        }
+        // window total sits in lane 0; it is older than what was accumulated so far
+        if (vh && lane == 0) {
+            if (SEG) {
+                if (!has) { acc = v; acc_head = hd; }
+                else if (!acc_head) { acc = (T)op(v, acc); acc_head = hd; }
+            } else {
+                acc = has ? (T)op(v, acc) : v;
+            }
+            has = true;
+        }
+        if (stop_mask) break;
+        j0 -= 32;
+    }
+    Opt<T> r;
+    r.v = shfl_any(acc, 0);
+    r.h = __shfl_sync(0xffffffffu, (int)has, 0) != 0;
+    seg_flag_out = __shfl_sync(0xffffffffu, (int)acc_head, 0) != 0;
+    return r;
+}
+
+template <class T>
+TRTC_FORCEINLINE void publish(const LookbackState& st, size_t tile, const T& v, bool inclusive, bool head) {
+    T* dst = reinterpret_cast<T*>(inclusive ? st.incl : st.agg);
+    dst[tile] = v;
+    if (st.heads) st.heads[tile] = head ? 1 : 0;
+    st_release(&st.flags[tile], st.epoch4 + (inclusive ? 2u : 1u));
+}
+
+TRTC_FORCEINLINE size_t claim_tile(const LookbackState& st, uint32_t* s_slot) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // tiles are handed out in launch order; the CTA that takes the last ticket resets
+        // the counter for the next launch on this stream (every ticket is already taken)
+        const unsigned long long t = atomicAdd(st.tile_ctr, 1ull);
+        if (t == (unsigned long long)gridDim.x - 1) atomicExch(st.tile_ctr, 0ull);
+        s_slot[0] = (uint32_t)t;
+        s_slot[1] = (uint32_t)(t >> 32);
+    }
+    __syncthreads();
+    return (size_t)s_slot[0] | ((size_t)s_slot[1] << 32);
+}
+
+// ---------------------------------------------------------------- scan kernel
+// Element (warp w, chunk v, lane l, e) of a tile is tile_base + w*NV*32*VEC + v*32*VEC +
+// l*VEC + e: a warp reads 32 consecutive 16-byte vectors per chunk (coalesced), and each
+// lane owns VEC consecutive elements, folded in registers before the warp-level scan.
+// MODE 0: inclusive.  MODE 1: exclusive with init (out[0] = init).  MODE 2: reduction only
+// (no output; the last tile stores the total in st.result).
+template <class InV, class UOp, bool HAS_UOP, class OutV, class T, class Op, int MODE, int BLOCK, int NV>
+__global__ void __launch_bounds__(BLOCK) scan_kernel(InV in, UOp uop, OutV out, size_t n, Op op, T init,
+                                                     LookbackState st) {
+    typedef ScanSrc<InV, T, UOp, HAS_UOP> Src;
+    Src src;
+    src.in = in;
+    src.uop = uop;
+    typedef typename Src::E E;
+    constexpr int VEC = Src::CONTIG ? VecWidth<E>::V : 1;
+    constexpr int WARPS = BLOCK / 32;
+    constexpr int TILE = BLOCK * NV * VEC;
+    __shared__ uint32_t s_slot[2];
+    __shared__ T s_wagg[WARPS];
+    __shared__ int s_whas[WARPS];
+    __shared__ T s_pre;
+    __shared__ int s_pre_has;
+
+    const size_t tile = claim_tile(st, s_slot);
+    const size_t tile_base = tile * TILE;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const size_t valid = (n - tile_base) < (size_t)TILE ? (n - tile_base) : (size_t)TILE;
+    const bool full = valid == (size_t)TILE;
+    const uint32_t woff = warp * (NV * 32 * VEC);
+
+    T x[NV][VEC];
+    // ---- load
+    bool vec_ok = false;
+    if constexpr (Src::CONTIG && VEC > 1) vec_ok = full && ((((size_t)src.in._data) & 15) == 0);
+    if (vec_ok) {
+        if constexpr (Src::CONTIG && VEC > 1) {
+            const uint4* p = reinterpret_cast<const uint4*>(src.in._data + tile_base + woff);
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                union { uint4 q; E e[VEC]; } u;
+                u.q = p[v * 32 + lane];
+#pragma unroll
+                for (int e = 0; e < VEC; e++) x[v][e] = src.get(u.e[e]);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+#pragma unroll
+            for (int e = 0; e < VEC; e++) {
+                const size_t r = woff + v * 32 * VEC + lane * VEC + e;
+                x[v][e] = (r < valid) ? src.get(src.fetch(tile_base + r)) : T();
+            }
+    }
+
+    // ---- thread folds + warp scans per chunk
+    T pre[NV];
+    bool pre_h[NV];
+    T carry = T();
+    bool carry_h = false;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        const long long cs = (long long)woff + v * 32 * VEC;             // chunk start in tile
+        const long long ls = cs + (long long)lane * VEC;                 // lane start
+        long long nvl = (long long)valid - ls;
+        nvl = nvl < 0 ? 0 : (nvl > VEC ? VEC : nvl);
+#pragma unroll
+        for (int e = 1; e < VEC; e++)
+            if (e < nvl) x[v][e] = (T)op(x[v][e - 1], x[v][e]);
+        const bool lane_valid = nvl > 0;
+        // last valid element of the lane (selected with constant indices: a runtime index
+        // would move the whole register array to local memory)
+        T inc = x[v][0];
+#pragma unroll
+        for (int e = 1; e < VEC; e++)
+            if (e < nvl) inc = x[v][e];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const T y = shfl_up_any(inc, d);
+            if ((int)lane >= d && lane_valid) inc = (T)op(y, inc);
+        }
+        const T ex = shfl_up_any(inc, 1);
+        const bool ex_h = lane > 0;
+        long long last_lane = ((long long)valid - cs - 1) / VEC;
+        if ((long long)valid - cs <= 0) last_lane = -1;
+        if (last_lane > 31) last_lane = 31;
+        const T ctot = shfl_any(inc, last_lane < 0 ? 0 : (int)last_lane);
+        pre[v] = carry;
+        pre_h[v] = carry_h;
+        opt_combine(pre[v], pre_h[v], ex, ex_h, op);
+        if (last_lane >= 0) opt_combine(carry, carry_h, ctot, true, op);
+    }
+    if (lane == 0) { s_wagg[warp] = carry; s_whas[warp] = carry_h ? 1 : 0; }
+    __syncthreads();
+
+    // ---- tile aggregate, look-back, prefixes
+    if (warp == 0) {
+        T agg = T();
+        bool agg_h = false;
+        if (lane == 0)
+            for (int w = 0; w < WARPS; w++) opt_combine(agg, agg_h, s_wagg[w], s_whas[w] != 0, op);
+        agg = shfl_any(agg, 0);
+        agg_h = __shfl_sync(0xffffffffu, (int)agg_h, 0) != 0;
+        T tp = T();
+        bool tp_h = false;
+        if (tile == 0) {
+            if (MODE == 1) { tp = init; tp_h = true; }
+            T incl = tp;
+            bool incl_h = tp_h;
+            opt_combine(incl, incl_h, agg, agg_h, op);
+            if (lane == 0) {
+                publish<T>(st, 0, incl, true, false);
+                if (MODE == 2 && valid == n && st.result) *reinterpret_cast<T*>(st.result) = incl;
+            }
+        } else {
+            if (lane == 0) publish<T>(st, tile, agg, false, false);
+            bool dummy;
+            const Opt<T> p = lookback_prefix<T, Op, false>(st, tile, op, dummy);
+            tp = p.v;
+            tp_h = p.h;
+            T incl = tp;
+            bool incl_h = tp_h;
+            opt_combine(incl, incl_h, agg, agg_h, op);
+            if (lane == 0) {
+                publish<T>(st, tile, incl, true, false);
+                if (MODE == 2 && tile_base + valid == n && st.result) *reinterpret_cast<T*>(st.result) = incl;
+            }
+        }
+        if (lane == 0) { s_pre = tp; s_pre_has = tp_h ? 1 : 0; }
+    }
+    if (MODE == 2) return;
+    __syncthreads();
+
+    // warp prefix = tile prefix ⊕ aggregates of earlier warps
+    T wp = s_pre;
+    bool wp_h = s_pre_has != 0;
+    for (uint32_t w = 0; w < warp; w++) opt_combine(wp, wp_h, s_wagg[w], s_whas[w] != 0, op);
+
+    // ---- outputs
+    bool st_vec = false;
+    if constexpr (ViewTraits<OutV>::contiguous && VEC > 1 && sizeof(T) == sizeof(E))
+        st_vec = vec_ok && ((((size_t)out._data) & 15) == 0) && out._size >= n;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        T tp = wp;
+        bool tp_h = wp_h;
+        opt_combine(tp, tp_h, pre[v], pre_h[v], op);
+        T y[VEC];
+#pragma unroll
+        for (int e = 0; e < VEC; e++) {
+            if (MODE == 0) {
+                y[e] = tp_h ? (T)op(tp, x[v][e]) : x[v][e];
+            } else {
+                y[e] = (e == 0) ? tp : (T)op(tp, x[v][e - 1]);
+            }
+        }
+        if constexpr (ViewTraits<OutV>::contiguous && VEC > 1 && sizeof(T) == sizeof(E)) {
+            if (st_vec) {
+                union { uint4 q; T t[VEC]; } u;
+#pragma unroll
+                for (int e = 0; e < VEC; e++) u.t[e] = y[e];
+                reinterpret_cast<uint4*>(out._data + tile_base + woff)[v * 32 + lane] = u.q;
+                continue;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < VEC; e++) {
+            const size_t r = woff + v * 32 * VEC + lane * VEC + e;
+            if (r < valid && tile_base + r < (size_t)out.size()) out[tile_base + r] = y[e];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- segmented scan kernel
+// Segments continue at i while pred(key[i-1], key[i]) (default EqualTo; a head starts a new
+// segment).  MODE 0: inclusive.  MODE 1: exclusive, out[head] = init, otherwise
+// init ⊕ (segment values before i).  Keys and values are read through their views.
+template <class KV, class InV, class OutV, class T, class Pred, class Op, int MODE, int BLOCK, int NV>
+__global__ void __launch_bounds__(BLOCK) scan_by_key_kernel(KV keys, InV vals, OutV out, size_t n, Pred pred, Op op,
+                                                           T init, LookbackState st) {
+    typedef ScanSrc<InV, T, Nothing, false> Src;
+    Src src;
+    src.in = vals;
+    typedef typename Src::E E;
+    typedef typename remove_cvref<typename KV::value_t>::type K;
+    constexpr bool CONTIG = Src::CONTIG && ViewTraits<KV>::contiguous && VecWidth<E>::V > 1 && VecWidth<K>::V > 1;
+    // lane chunk width: 16 bytes of the narrower type (the wider one takes several vectors)
+    constexpr int VEC = CONTIG ? (VecWidth<E>::V > VecWidth<K>::V ? VecWidth<E>::V : VecWidth<K>::V) : 1;
+    constexpr int WARPS = BLOCK / 32;
+    constexpr int TILE = BLOCK * NV * VEC;
+    __shared__ uint32_t s_slot[2];
+    __shared__ T s_wagg[WARPS];
+    __shared__ int s_whas[WARPS], s_whd[WARPS];
+    __shared__ T s_pre;
+    __shared__ int s_pre_has, s_pre_hd;
+
+    const size_t tile = claim_tile(st, s_slot);
+    const size_t tile_base = tile * TILE;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const size_t valid = (n - tile_base) < (size_t)TILE ? (n - tile_base) : (size_t)TILE;
+    const bool full = valid == (size_t)TILE;
+    const uint32_t woff = warp * (NV * 32 * VEC);
+
+    T x[NV][VEC];
+    K k[NV][VEC];
+    bool vec_ok = false;
+    if constexpr (CONTIG && VEC > 1)
+        vec_ok = full && ((((size_t)src.in._data) & 15) == 0) && ((((size_t)keys._data) & 15) == 0);
+    if (vec_ok) {
+        if constexpr (CONTIG && VEC > 1) {
+            constexpr int KV4 = VEC * (int)sizeof(K) / 16;  // 16-byte vectors of keys per chunk-lane
+            constexpr int EV4 = VEC * (int)sizeof(E) / 16;
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                const size_t r0 = tile_base + woff + v * 32 * VEC + lane * VEC;
+                union { uint4 q[KV4 > 0 ? KV4 : 1]; K e[VEC]; } uk;
+                union { uint4 q[EV4 > 0 ? EV4 : 1]; E e[VEC]; } ue;
+#pragma unroll
+                for (int q = 0; q < KV4; q++) uk.q[q] = reinterpret_cast<const uint4*>(keys._data + r0)[q];
+#pragma unroll
+                for (int q = 0; q < EV4; q++) ue.q[q] = reinterpret_cast<const uint4*>(src.in._data + r0)[q];
+#pragma unroll
+                for (int e = 0; e < VEC; e++) { k[v][e] = uk.e[e]; x[v][e] = src.get(ue.e[e]); }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+#pragma unroll
+            for (int e = 0; e < VEC; e++) {
+                const size_t r = woff + v * 32 * VEC + lane * VEC + e;
+                if (r < valid) { k[v][e] = keys[tile_base + r]; x[v][e] = src.get(src.fetch(tile_base + r)); }
+                else { k[v][e] = K(); x[v][e] = T(); }
+            }
+    }
+
+    // heads: compare with the previous element's key
+    bool h[NV][VEC];
+    K carry_key = K();
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        const size_t ls = woff + v * 32 * VEC + lane * VEC;
+        K prev = shfl_up_any(k[v][VEC - 1], 1);
+        const K last31 = shfl_any(k[v][VEC - 1], 31);
+        if (lane == 0) {
+            if (v > 0) prev = carry_key;
+            else if (tile_base + ls > 0 && tile_base + ls - 1 < n) prev = keys[tile_base + ls - 1];
+        }
+        carry_key = last31;
+#pragma unroll
+        for (int e = 0; e < VEC; e++) {
+            const size_t gi = tile_base + ls + e;
+            const K pk = e == 0 ? prev : k[v][e - 1];
+            h[v][e] = (gi == 0) || !pred(pk, k[v][e]);
+        }
+    }
+
+    // thread folds + segmented warp scans
+    T pre[NV];
+    bool pre_h[NV], pre_hd[NV];
+    T xin[NV][VEC];  // inclusive value of each element within its thread chunk
+    T carry = T();
+    bool carry_h = false, carry_hd = false;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        const long long cs = (long long)woff + v * 32 * VEC;
+        const long long ls = cs + (long long)lane * VEC;
+        long long nvl = (long long)valid - ls;
+        nvl = nvl < 0 ? 0 : (nvl > VEC ? VEC : nvl);
+        bool thd = h[v][0];
+        xin[v][0] = x[v][0];
+#pragma unroll
+        for (int e = 1; e < VEC; e++) {
+            xin[v][e] = (e < nvl && !h[v][e]) ? (T)op(xin[v][e - 1], x[v][e]) : x[v][e];
+            if (e < nvl) thd = thd || h[v][e];
+        }
+        const bool lane_valid = nvl > 0;
+        T inc = xin[v][0];
+#pragma unroll
+        for (int e = 1; e < VEC; e++)
+            if (e < nvl) inc = xin[v][e];
+        bool ihd = thd;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const T y = shfl_up_any(inc, d);
+            const int yhd = __shfl_up_sync(0xffffffffu, (int)ihd, d);
+            if ((int)lane >= d && lane_valid) {
+                if (!ihd) inc = (T)op(y, inc);
+                ihd = ihd || yhd;
+            }
+        }
+        const T ex = shfl_up_any(inc, 1);
+        const int exhd = __shfl_up_sync(0xffffffffu, (int)ihd, 1);
+        long long last_lane = ((long long)valid - cs - 1) / VEC;
+        if ((long long)valid - cs <= 0) last_lane = -1;
+        if (last_lane > 31) last_lane = 31;
+        const int ll = last_lane < 0 ? 0 : (int)last_lane;
+        const T ctot = shfl_any(inc, ll);
+        const int ctothd = __shfl_sync(0xffffffffu, (int)ihd, ll);
+        // thread prefix = carry ⊕seg ex
+        pre[v] = carry; pre_h[v] = carry_h; pre_hd[v] = carry_hd;
+        if (lane > 0) {
+            if (!pre_h[v] || exhd) { pre[v] = ex; pre_hd[v] = exhd || (pre_h[v] && pre_hd[v]); }
+            else { pre[v] = (T)op(pre[v], ex); }
+            pre_h[v] = true;
+        }
+        if (last_lane >= 0) {
+            if (!carry_h || ctothd) { carry = ctot; carry_hd = ctothd || (carry_h && carry_hd); }
+            else carry = (T)op(carry, ctot);
+            carry_h = true;
+        }
+    }
+    if (lane == 0) { s_wagg[warp] = carry; s_whas[warp] = carry_h ? 1 : 0; s_whd[warp] = carry_hd ? 1 : 0; }
+    __syncthreads();
+
+    if (warp == 0) {
+        T agg = T();
+        bool agg_h = false, agg_hd = false;
+        if (lane == 0)
+            for (int w = 0; w < WARPS; w++) {
+                if (!s_whas[w]) continue;
+                if (!agg_h || s_whd[w]) { agg = s_wagg[w]; agg_hd = s_whd[w] || (agg_h && agg_hd); }
+                else agg = (T)op(agg, s_wagg[w]);
+                agg_h = true;
+            }
+        agg = shfl_any(agg, 0);
+        agg_h = __shfl_sync(0xffffffffu, (int)agg_h, 0) != 0;
+        agg_hd = __shfl_sync(0xffffffffu, (int)agg_hd, 0) != 0;
+        T tp = T();
+        bool tp_h = false, tp_hd = false;
+        if (tile > 0) {
+            if (lane == 0) publish<T>(st, tile, agg, false, agg_hd);
+            const Opt<T> p = lookback_prefix<T, Op, true>(st, tile, op, tp_hd);
+            tp = p.v;
+            tp_h = p.h;
+        }
+        // inclusive of this tile = tp ⊕seg agg
+        T incl = tp;
+        bool incl_hd = tp_hd;
+        if (!tp_h || agg_hd) { incl = agg; incl_hd = agg_hd || (tp_h && tp_hd); }
+        else incl = (T)op(tp, agg);
+        if (lane == 0) {
+            publish<T>(st, tile, incl, true, incl_hd);
+            s_pre = tp; s_pre_has = tp_h ? 1 : 0; s_pre_hd = tp_hd ? 1 : 0;
+        }
+    }
+    __syncthreads();
+
+    T wp = s_pre;
+    bool wp_h = s_pre_has != 0;
+    for (uint32_t w = 0; w < warp; w++) {
+        if (!s_whas[w]) continue;
+        if (!wp_h || s_whd[w]) wp = s_wagg[w];
+        else wp = (T)op(wp, s_wagg[w]);
+        wp_h = true;
+    }
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        // thread prefix (running inclusive value of the element before this lane's first)
+        T tp = wp;
+        bool tp_h = wp_h;
+        if (pre_h[v]) {
+            if (!tp_h || pre_hd[v]) tp = pre[v];
+            else tp = (T)op(tp, pre[v]);
+            tp_h = true;
+        }
+        T run = tp;  // inclusive value of the previous element
+#pragma unroll
+        for (int e = 0; e < VEC; e++) {
+            const size_t r = woff + v * 32 * VEC + lane * VEC + e;
+            T cur;  // inclusive value of this element
+            if (h[v][e]) cur = x[v][e];
+            else if (e == 0) cur = tp_h ? (T)op(tp, x[v][e]) : x[v][e];
+            else cur = (T)op(run, x[v][e]);
+            T y;
+            if (MODE == 0) y = cur;
+            else y = h[v][e] ? init : (T)op(init, run);
+            run = cur;
+            if (r < valid && tile_base + r < (size_t)out.size()) out[tile_base + r] = y;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- commutative reduce
+// Built-in commutative operators over contiguous input: 16-byte loads, VEC independent
+// per-thread accumulators (shorter FP accumulation chains), warp/block trees, one partial
+// per CTA, and the last CTA to finish folds the partials (no second launch).
+template <class E, class T, class Op, class UOp, bool HAS_UOP, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) reduce_kernel(const E* __restrict__ in, size_t n, Op op, UOp uop, T* partials,
+                                                       int* partial_has, uint32_t* done_ctr, T* result, int has_init,
+                                                       T init) {
+    constexpr int VEC = VecWidth<E>::V;
+    constexpr int WARPS = BLOCK / 32;
+    __shared__ T s_w[WARPS];
+    __shared__ int s_wh[WARPS];
+    __shared__ bool s_last;
+    auto get = [&](const E& e) -> T {
+        if constexpr (HAS_UOP) return (T)uop(e);
+        else return (T)e;
+    };
+    T acc[VEC];
+    bool acc_h = false;
+    const bool aligned = ((((size_t)in) & 15) == 0);
+    const size_t nvec = aligned ? n / VEC : 0;
+    const size_t gtid = (size_t)blockIdx.x * BLOCK + threadIdx.x, gsz = (size_t)gridDim.x * BLOCK;
+    size_t vi = gtid;
+    if (vi < nvec) {
+        union { uint4 q; E e[VEC]; } u;
+        u.q = reinterpret_cast<const uint4*>(in)[vi];
+#pragma unroll
+        for (int e = 0; e < VEC; e++) acc[e] = get(u.e[e]);
+        acc_h = true;
+        for (vi += gsz; vi < nvec; vi += gsz) {
+            u.q = reinterpret_cast<const uint4*>(in)[vi];
+#pragma unroll
+            for (int e = 0; e < VEC; e++) acc[e] = (T)op(acc[e], get(u.e[e]));
+        }
+    }
+    T a = acc[0];
+    if (acc_h) {
+#pragma unroll
+        for (int e = 1; e < VEC; e++) a = (T)op(a, acc[e]);
+    }
+    for (size_t i = nvec * VEC + gtid; i < n; i += gsz) {
+        const T t = get(in[i]);
+        a = acc_h ? (T)op(a, t) : t;
+        acc_h = true;
+    }
+    // warp tree
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        const T o = shfl_down_any(a, d);
+        const int oh = __shfl_down_sync(0xffffffffu, (int)acc_h, d);
+        if ((int)lane_id() + d < 32 && oh) { a = acc_h ? (T)op(a, o) : o; acc_h = true; }
+    }
+    const uint32_t warp = threadIdx.x >> 5;
+    if (lane_id() == 0) { s_w[warp] = a; s_wh[warp] = acc_h ? 1 : 0; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T b = T();
+        bool bh = false;
+        for (int w = 0; w < WARPS; w++) opt_combine(b, bh, s_w[w], s_wh[w] != 0, op);
+        partials[blockIdx.x] = b;
+        partial_has[blockIdx.x] = bh ? 1 : 0;
+        __threadfence();
+        const uint32_t prev = atomicAdd(done_ctr, 1u);
+        s_last = prev == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        T r = init;
+        bool rh = has_init != 0;
+        for (uint32_t b = 0; b < gridDim.x; b++) {
+            const T p = *(volatile T*)&partials[b];
+            const int ph = *(volatile int*)&partial_has[b];
+            opt_combine(r, rh, p, ph != 0, op);
+        }
+        *result = r;
+        *done_ctr = 0;  // leaves the counter ready for the next call
+    }
+}
+
+}  // namespace trtc

@@ -1,0 +1,91 @@
+// api_raw.cpp -- raw-pointer C ABI (include/trtc_raw.h): built-in element types on device
+// buffers the caller owns, on a caller-chosen stream.  The object-model ABI of
+// include/thrustrtc_b200.h is layered on the same launchers.
+#include "trtc_launch.h"
+#include "trtc_runtime.h"
+
+using namespace trtc_host;
+
+static inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+extern "C" {
+
+const char* trtc_last_error() { return last_error(); }
+
+unsigned long long trtc_launch_count() { return launch_count(); }
+
+// Copies the sort control block of `stream` (histograms, plan, NaN flag, rotation count of
+// the last sort on that stream) to host memory; for diagnostics.  Returns bytes copied.
+unsigned long long trtc_debug_sort_ctrl(void* host, unsigned long long bytes, void* stream) {
+    void* c = sort_ctrl_ws(S(stream), 1 << 16);
+    if (!c || !host) return 0;
+    if (!TRTC_CUDA(cudaMemcpyAsync(host, c, (size_t)bytes, cudaMemcpyDeviceToHost, S(stream)))) return 0;
+    if (!TRTC_CUDA(cudaStreamSynchronize(S(stream)))) return 0;
+    return bytes;
+}
+
+int trtc_raw_sync(void* stream) {
+    if (!ensure_device()) return -1;
+    return check_device_errors(S(stream), "stream") ? 0 : -1;
+}
+
+int trtc_raw_sort(int key_tc, void* keys, unsigned long long n, int descending, void* stream) {
+    if (!ensure_device()) return -1;
+    return sort_raw(key_tc, keys, nullptr, 0, (size_t)n, descending != 0, S(stream)) ? 0 : -1;
+}
+
+int trtc_raw_sort_by_key(int key_tc, void* keys, void* values, unsigned long long value_size, unsigned long long n,
+                         int descending, void* stream) {
+    if (!ensure_device()) return -1;
+    if (!values || value_size == 0) { set_error("sort_by_key: no values"); return -1; }
+    return sort_raw(key_tc, keys, values, (size_t)value_size, (size_t)n, descending != 0, S(stream)) ? 0 : -1;
+}
+
+unsigned long long trtc_raw_min_element(int tc, const void* in, unsigned long long n, void* stream) {
+    if (!ensure_device()) return ~0ull;
+    unsigned long long idx = 0;
+    return min_element_raw(tc, in, (size_t)n, S(stream), &idx) ? idx : ~0ull;
+}
+
+int trtc_raw_scan(int tc, int op, int exclusive, const void* in, void* out, unsigned long long n, const void* init,
+                  void* stream) {
+    if (!ensure_device()) return -1;
+    if (exclusive && !init) {
+        static const unsigned long long zero[2] = {0, 0};
+        init = zero;
+    }
+    return scan_raw(tc, op, exclusive ? 1 : 0, in, out, (size_t)n, init, S(stream)) ? 0 : -1;
+}
+
+int trtc_raw_reduce(int tc, int op, const void* in, unsigned long long n, const void* init, void* result_host,
+                    void* stream) {
+    if (!ensure_device()) return -1;
+    return reduce_raw(tc, op, in, (size_t)n, init, result_host, S(stream)) ? 0 : -1;
+}
+
+int trtc_raw_reduce_async(int tc, int op, const void* in, unsigned long long n, const void* init, void** result_dev,
+                          void* stream) {
+    if (!ensure_device()) return -1;
+    return reduce_raw_async(tc, op, in, (size_t)n, init, result_dev, S(stream)) ? 0 : -1;
+}
+
+int trtc_raw_scan_by_key(int key_tc, int val_tc, int exclusive, const void* keys, const void* vals, void* out,
+                         unsigned long long n, const void* init, void* stream) {
+    if (!ensure_device()) return -1;
+    return scan_by_key_raw(key_tc, val_tc, exclusive ? 1 : 0, keys, vals, out, (size_t)n, init, S(stream)) ? 0 : -1;
+}
+
+unsigned long long trtc_raw_remove_copy(int tc, const void* in, void* out, unsigned long long n, const void* value,
+                                        void* stream) {
+    if (!ensure_device()) return ~0ull;
+    unsigned long long c = 0;
+    return compact_raw(tc, COMPACT_NOT_EQUAL, in, out, (size_t)n, value, S(stream), &c) ? c : ~0ull;
+}
+
+unsigned long long trtc_raw_unique_copy(int tc, const void* in, void* out, unsigned long long n, void* stream) {
+    if (!ensure_device()) return ~0ull;
+    unsigned long long c = 0;
+    return compact_raw(tc, COMPACT_UNIQUE, in, out, (size_t)n, nullptr, S(stream), &c) ? c : ~0ull;
+}
+
+}  // extern "C"

@@ -1,0 +1,225 @@
+// launch_scan.cu -- nvcc instantiations of the scan / reduce / scan_by_key / compaction
+// kernels for the built-in element types and operators (Plus, Maximum, Minimum, EqualTo).
+#include "trtc_launch.h"
+#include "trtc_runtime.h"
+#include "../device/trtc_compact.cuh"
+
+namespace trtc_host {
+
+using namespace trtc;
+
+static constexpr int SCAN_BLOCK = 256;
+
+template <class E> static constexpr int scan_nv() { return VecWidth<E>::V >= 16 ? 1 : 16 / VecWidth<E>::V; }
+
+static bool fill_lookback(LookbackState& st, cudaStream_t s, size_t tiles, size_t vsize, bool seg = false) {
+    uint32_t e4 = 0;
+    LookbackWs* w = lookback_ws(s, tiles, vsize, &e4);
+    if (!w) return false;
+    st.flags = w->flags;
+    st.agg = w->agg;
+    st.incl = w->incl;
+    st.heads = seg ? w->heads : nullptr;
+    st.tile_ctr = w->tile_ctr;
+    st.epoch4 = e4;
+    st.err = device_error_word();
+    st.result = w->result;
+    return true;
+}
+
+template <class T, class Op, int MODE>
+static bool scan_t(const T* in, T* out, size_t n, const T* init, cudaStream_t s) {
+    constexpr int NV = scan_nv<T>();
+    constexpr int TILE = SCAN_BLOCK * NV * VecWidth<T>::V;
+    const size_t tiles = (n + TILE - 1) / TILE;
+    LookbackState st;
+    if (!fill_lookback(st, s, tiles, sizeof(T))) return false;
+    VectorView<T> iv = make_view<T>(const_cast<T*>(in), n);
+    VectorView<T> ov = make_view<T>(out, n);
+    T ini = init ? *init : T();
+    scan_kernel<VectorView<T>, Nothing, false, VectorView<T>, T, Op, MODE, SCAN_BLOCK, NV>
+        <<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(iv, Nothing(), ov, n, Op(), ini, st);
+    count_launch();
+    return TRTC_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static bool scan_op(int op, int mode, const void* in, void* out, size_t n, const void* init, cudaStream_t s) {
+    const T* i = (const T*)in;
+    T* o = (T*)out;
+    const T* ini = (const T*)init;
+    switch (op * 2 + mode) {
+        case 0: return scan_t<T, Plus, 0>(i, o, n, ini, s);
+        case 1: return scan_t<T, Plus, 1>(i, o, n, ini, s);
+        case 2: return scan_t<T, Maximum, 0>(i, o, n, ini, s);
+        case 3: return scan_t<T, Maximum, 1>(i, o, n, ini, s);
+        case 4: return scan_t<T, Minimum, 0>(i, o, n, ini, s);
+        case 5: return scan_t<T, Minimum, 1>(i, o, n, ini, s);
+        default: set_error("scan: unsupported operator"); return false;
+    }
+}
+
+bool scan_raw(int tc, int op, int mode, const void* in, void* out, size_t n, const void* init, cudaStream_t s) {
+    if (n == 0) { set_error("scan: empty input"); return false; }
+    switch (tc) {
+        case TC_I8: return scan_op<int8_t>(op, mode, in, out, n, init, s);
+        case TC_U8: return scan_op<uint8_t>(op, mode, in, out, n, init, s);
+        case TC_I16: return scan_op<int16_t>(op, mode, in, out, n, init, s);
+        case TC_U16: return scan_op<uint16_t>(op, mode, in, out, n, init, s);
+        case TC_I32: return scan_op<int32_t>(op, mode, in, out, n, init, s);
+        case TC_U32: return scan_op<uint32_t>(op, mode, in, out, n, init, s);
+        case TC_I64: return scan_op<int64_t>(op, mode, in, out, n, init, s);
+        case TC_U64: return scan_op<uint64_t>(op, mode, in, out, n, init, s);
+        case TC_F32: return scan_op<float>(op, mode, in, out, n, init, s);
+        case TC_F64: return scan_op<double>(op, mode, in, out, n, init, s);
+        default: set_error("scan: unsupported type"); return false;
+    }
+}
+
+// ---------------------------------------------------------------- reduce
+template <class T, class Op>
+static bool reduce_t(const T* in, size_t n, const T* init, void** result_dev, cudaStream_t s) {
+    constexpr int BLOCK = 256;
+    const size_t nvec = n / VecWidth<T>::V;
+    size_t grid = (nvec + BLOCK - 1) / BLOCK;
+    const size_t cap = (size_t)sm_count() * 8;
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    LookbackWs* w = reduce_ws(s, grid, sizeof(T));
+    if (!w) return false;
+    reduce_kernel<T, T, Op, Identity, false, BLOCK><<<(unsigned)grid, BLOCK, 0, s>>>(
+        in, n, Op(), Identity(), (T*)w->partials, w->partial_has, w->done_ctr, (T*)w->result, init ? 1 : 0,
+        init ? *init : T());
+    count_launch();
+    *result_dev = w->result;
+    return TRTC_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static bool reduce_op(int op, const void* in, size_t n, const void* init, void** res, cudaStream_t s) {
+    switch (op) {
+        case OP_PLUS: return reduce_t<T, Plus>((const T*)in, n, (const T*)init, res, s);
+        case OP_MAX: return reduce_t<T, Maximum>((const T*)in, n, (const T*)init, res, s);
+        case OP_MIN: return reduce_t<T, Minimum>((const T*)in, n, (const T*)init, res, s);
+        default: set_error("reduce: unsupported operator"); return false;
+    }
+}
+
+bool reduce_raw_async(int tc, int op, const void* in, size_t n, const void* init, void** res, cudaStream_t s) {
+    if (n == 0 && !init) { set_error("reduce: empty input without an initial value"); return false; }
+    switch (tc) {
+        case TC_I8: return reduce_op<int8_t>(op, in, n, init, res, s);
+        case TC_U8: return reduce_op<uint8_t>(op, in, n, init, res, s);
+        case TC_I16: return reduce_op<int16_t>(op, in, n, init, res, s);
+        case TC_U16: return reduce_op<uint16_t>(op, in, n, init, res, s);
+        case TC_I32: return reduce_op<int32_t>(op, in, n, init, res, s);
+        case TC_U32: return reduce_op<uint32_t>(op, in, n, init, res, s);
+        case TC_I64: return reduce_op<int64_t>(op, in, n, init, res, s);
+        case TC_U64: return reduce_op<uint64_t>(op, in, n, init, res, s);
+        case TC_F32: return reduce_op<float>(op, in, n, init, res, s);
+        case TC_F64: return reduce_op<double>(op, in, n, init, res, s);
+        default: set_error("reduce: unsupported type"); return false;
+    }
+}
+
+bool reduce_raw(int tc, int op, const void* in, size_t n, const void* init, void* result_host, cudaStream_t s) {
+    void* rd = nullptr;
+    if (!reduce_raw_async(tc, op, in, n, init, &rd, s)) return false;
+    return TRTC_CUDA(cudaMemcpyAsync(result_host, rd, type_size(tc), cudaMemcpyDeviceToHost, s)) &&
+           check_device_errors(s, "reduce");
+}
+
+// ---------------------------------------------------------------- scan_by_key
+template <class K, class T, int MODE>
+static bool sbk_t(const K* keys, const T* vals, T* out, size_t n, const T* init, cudaStream_t s) {
+    constexpr int VK = VecWidth<K>::V, VT = VecWidth<T>::V;
+    constexpr int VEC = VK > VT ? VK : VT;
+    constexpr int NV = VEC >= 8 ? 2 : 4;
+    constexpr int TILE = SCAN_BLOCK * NV * VEC;
+    const size_t tiles = (n + TILE - 1) / TILE;
+    LookbackState st;
+    if (!fill_lookback(st, s, tiles, sizeof(T), true)) return false;
+    VectorView<T> vv = make_view<T>(const_cast<T*>(vals), n);
+    VectorView<K> kv = make_view<K>(const_cast<K*>(keys), n);
+    VectorView<T> ov = make_view<T>(out, n);
+    scan_by_key_kernel<VectorView<K>, VectorView<T>, VectorView<T>, T, EqualTo, Plus, MODE, SCAN_BLOCK, NV>
+        <<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(kv, vv, ov, n, EqualTo(), Plus(), init ? *init : T(), st);
+    count_launch();
+    return TRTC_CUDA(cudaGetLastError());
+}
+
+template <class K>
+static bool sbk_k(int vtc, int mode, const void* keys, const void* vals, void* out, size_t n, const void* init,
+                  cudaStream_t s) {
+    const K* k = (const K*)keys;
+#define TRTC_SBK(T) return mode ? sbk_t<K, T, 1>(k, (const T*)vals, (T*)out, n, (const T*)init, s) \
+                                : sbk_t<K, T, 0>(k, (const T*)vals, (T*)out, n, (const T*)init, s)
+    switch (vtc) {
+        case TC_I32: TRTC_SBK(int32_t);
+        case TC_U32: TRTC_SBK(uint32_t);
+        case TC_I64: TRTC_SBK(int64_t);
+        case TC_F32: TRTC_SBK(float);
+        case TC_F64: TRTC_SBK(double);
+        default: set_error("scan_by_key: unsupported value type"); return false;
+    }
+#undef TRTC_SBK
+}
+
+bool scan_by_key_raw(int ktc, int vtc, int mode, const void* keys, const void* vals, void* out, size_t n,
+                     const void* init, cudaStream_t s) {
+    if (n == 0) { set_error("scan_by_key: empty input"); return false; }
+    switch (ktc) {
+        case TC_I32: return sbk_k<int32_t>(vtc, mode, keys, vals, out, n, init, s);
+        case TC_U32: return sbk_k<uint32_t>(vtc, mode, keys, vals, out, n, init, s);
+        case TC_I64: return sbk_k<int64_t>(vtc, mode, keys, vals, out, n, init, s);
+        default: set_error("scan_by_key: unsupported key type"); return false;
+    }
+}
+
+// ---------------------------------------------------------------- compaction (built-in selectors)
+template <class T, int MODE>
+static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_t s, unsigned long long* count) {
+    constexpr int ITEMS = 16;
+    constexpr int TILE = SCAN_BLOCK * ITEMS;
+    const size_t tiles = (n + TILE - 1) / TILE;
+    LookbackState st;
+    if (!fill_lookback(st, s, tiles, 8)) return false;
+    VectorView<T> iv = make_view<T>(const_cast<T*>(in), n);
+    VectorView<T> ov = make_view<T>(out, n);
+    compact_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing, Nothing, Nothing,
+                   SCAN_BLOCK, ITEMS><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(
+        iv, Nothing(), EqualTo(), value ? *value : T(), ov, Nothing(), Nothing(), Nothing(), n, st);
+    count_launch();
+    if (!TRTC_CUDA(cudaGetLastError())) return false;
+    return TRTC_CUDA(cudaMemcpyAsync(count, st.result, 8, cudaMemcpyDeviceToHost, s)) &&
+           check_device_errors(s, "compaction");
+}
+
+template <class T>
+static bool compact_m(int mode, const void* in, void* out, size_t n, const void* value, cudaStream_t s,
+                      unsigned long long* count) {
+    if (mode == CM_NOT_EQUAL) return compact_t<T, CM_NOT_EQUAL>((const T*)in, (T*)out, n, (const T*)value, s, count);
+    if (mode == CM_UNIQUE) return compact_t<T, CM_UNIQUE>((const T*)in, (T*)out, n, nullptr, s, count);
+    set_error("compaction: unsupported built-in mode");
+    return false;
+}
+
+bool compact_raw(int tc, int mode, const void* in, void* out, size_t n, const void* value, cudaStream_t s,
+                 unsigned long long* count) {
+    if (n == 0) { set_error("compaction: empty input"); return false; }
+    switch (tc) {
+        case TC_I8: return compact_m<int8_t>(mode, in, out, n, value, s, count);
+        case TC_U8: return compact_m<uint8_t>(mode, in, out, n, value, s, count);
+        case TC_I16: return compact_m<int16_t>(mode, in, out, n, value, s, count);
+        case TC_U16: return compact_m<uint16_t>(mode, in, out, n, value, s, count);
+        case TC_I32: return compact_m<int32_t>(mode, in, out, n, value, s, count);
+        case TC_U32: return compact_m<uint32_t>(mode, in, out, n, value, s, count);
+        case TC_I64: return compact_m<int64_t>(mode, in, out, n, value, s, count);
+        case TC_U64: return compact_m<uint64_t>(mode, in, out, n, value, s, count);
+        case TC_F32: return compact_m<float>(mode, in, out, n, value, s, count);
+        case TC_F64: return compact_m<double>(mode, in, out, n, value, s, count);
+        default: set_error("compaction: unsupported type"); return false;
+    }
+}
+
+}  // namespace trtc_host
