@@ -1,0 +1,58 @@
+/* trtc_raw.h -- raw-pointer entry points of libPyThrustRTC.so (thrustrtc_b200 additions).
+ *
+ * These have no counterpart in the reference's python/api.h: they run the same nvcc-built
+ * kernels on caller-owned device buffers of the built-in element types, on a caller-chosen
+ * CUDA stream (void* = cudaStream_t, NULL = legacy default stream), without the object
+ * model.  They back the benchmark, the batched and serving paths, and direct C users.
+ * Element type codes: 0 int8, 1 uint8, 2 int16, 3 uint16, 4 int32, 5 uint32, 6 int64,
+ * 7 uint64, 8 float, 9 double.  Operator codes: 0 Plus, 1 Maximum, 2 Minimum.
+ * int results: 0 success, -1 failure (trtc_last_error() describes it).  Calls that return
+ * a count or value synchronise the stream; the others are asynchronous, and trtc_raw_sync()
+ * synchronises and reports any device-side error (e.g. an exceeded bounded wait).
+ */
+#ifndef TRTC_RAW_H
+#define TRTC_RAW_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+const char* trtc_last_error(void);
+/* number of thrustrtc_b200 kernels launched by this process */
+unsigned long long trtc_launch_count(void);
+/* synchronises `stream`; 0, or -1 when a kernel reported an error */
+int trtc_raw_sync(void* stream);
+
+/* stable radix sort in place; same order as TRTC_Sort with Less (descending=0) or Greater */
+int trtc_raw_sort(int key_type, void* keys, unsigned long long n, int descending, void* stream);
+/* pairs: values of `value_size` bytes move with their keys */
+int trtc_raw_sort_by_key(int key_type, void* keys, void* values, unsigned long long value_size,
+                         unsigned long long n, int descending, void* stream);
+/* index selected by TRTC_Min_Element's reduction tree (~0ull on failure); synchronous */
+unsigned long long trtc_raw_min_element(int type, const void* in, unsigned long long n, void* stream);
+
+/* inclusive (exclusive=0) or exclusive scan with host-side init (NULL: zero) */
+int trtc_raw_scan(int type, int op, int exclusive, const void* in, void* out, unsigned long long n,
+                  const void* init, void* stream);
+/* reduction to host memory (init may be NULL); synchronous */
+int trtc_raw_reduce(int type, int op, const void* in, unsigned long long n, const void* init, void* result_host,
+                    void* stream);
+/* reduction left in device memory at *result_dev (library-owned, valid until the next call) */
+int trtc_raw_reduce_async(int type, int op, const void* in, unsigned long long n, const void* init,
+                          void** result_dev, void* stream);
+/* segmented scan, EqualTo keys / Plus values */
+int trtc_raw_scan_by_key(int key_type, int value_type, int exclusive, const void* keys, const void* values,
+                         void* out, unsigned long long n, const void* init, void* stream);
+/* stable compactions; return the number of elements written (~0ull on failure) */
+unsigned long long trtc_raw_remove_copy(int type, const void* in, void* out, unsigned long long n,
+                                        const void* value, void* stream);
+unsigned long long trtc_raw_unique_copy(int type, const void* in, void* out, unsigned long long n, void* stream);
+
+/* diagnostics: copies the sort control block of the last sort on `stream` */
+unsigned long long trtc_debug_sort_ctrl(void* host, unsigned long long bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TRTC_RAW_H */

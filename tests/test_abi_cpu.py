@@ -1,0 +1,51 @@
+"""The C-ABI library loads without a GPU and exports every entry point include/*.h declares."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "thrustrtc_b200", "libPyThrustRTC.so")
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b((?:n|trtc)_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def exported():
+    assert os.path.exists(LIB), "build the library first (python -m thrustrtc_b200.build)"
+    out = subprocess.check_output(["nm", "-D", "--defined-only", LIB]).decode()
+    return set(line.split()[-1] for line in out.splitlines() if line.strip())
+
+
+@pytest.mark.parametrize("header", ["thrustrtc_b200.h", "trtc_raw.h"])
+def test_every_declared_symbol_is_exported(header, exported):
+    names = _declared(header)
+    assert names, header
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+
+
+def test_library_loads_without_gpu():
+    lib = ctypes.CDLL(LIB)
+    lib.trtc_launch_count.restype = ctypes.c_ulonglong
+    assert lib.trtc_launch_count() == 0
+
+
+def test_python_package_imports():
+    import thrustrtc_b200 as trtc
+    assert hasattr(trtc, "Sort_By_Key") and hasattr(trtc, "Inclusive_Scan") and hasattr(trtc, "Copy_If")
+
+
+def test_no_exit_calls_in_library():
+    # a host-side call of a device-only helper compiles into exit(1); none may be present
+    try:
+        dis = subprocess.check_output(["objdump", "-d", "--no-show-raw-insn", LIB], stderr=subprocess.DEVNULL).decode()
+    except (OSError, subprocess.CalledProcessError):
+        pytest.skip("objdump not available")
+    assert "<exit@plt>" not in "\n".join(l for l in dis.splitlines() if "call" in l)

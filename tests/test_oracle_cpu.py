@@ -1,0 +1,119 @@
+"""CPU checks of the oracle itself, against the reference's golden vectors.
+
+Pins: docs/QuickStartGuide.md known answers (tests/golden/docs_vectors.json), the
+self-checking big cases of cpp/test/test_sort.cpp (tests/golden/test_sort_cpp.npz), and
+d_u32/d_u64 + Maximum/Minimum evaluated by the reference's own built_in.h compiled on the
+CPU (tests/golden/builtin_h_probe.json).  Also cross-checks the oracle's fast sort against
+its literal restatement of the 1-bit LSD split.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+NP = {"int32_t": np.int32, "int8_t": np.int8}
+
+
+def _docs():
+    with open(os.path.join(GOLD, "docs_vectors.json")) as f:
+        return json.load(f)
+
+
+def test_docs_scans():
+    d = _docs()
+    x = np.array(d["inclusive_scan"]["in"], np.int32)
+    assert O.scan(x).tolist() == d["inclusive_scan"]["out"]
+    x = np.array(d["exclusive_scan"]["in"], np.int32)
+    assert O.scan(x, exclusive=True).tolist() == d["exclusive_scan"]["out"]
+
+
+def test_docs_sorts():
+    d = _docs()
+    x = np.array(d["sort"]["in"], np.int32)
+    assert O.sort(x).tolist() == d["sort"]["out"]
+    assert O.sort(x, descending=True).tolist() == d["sort_greater"]["out"]
+    for case in ("sort_by_key_char", "sort_by_key_int"):
+        c = d[case]
+        k, v = O.sort_by_key(np.array(c["keys"], NP[c["key_dtype"]]), np.array(c["values"], NP[c["value_dtype"]]))
+        assert k.tolist() == c["keys_out"] and v.tolist() == c["values_out"]
+
+
+def test_reference_test_sort_bigcases():
+    g = np.load(os.path.join(GOLD, "test_sort_cpp.npz"))
+    assert (O.sort(g["sort_in"]) == np.arange(1, 10001)).all()
+    k, v = O.sort_by_key(g["sbk_keys"], g["sbk_values"])
+    assert (k == np.arange(1, 10001)).all() and (v == 10000 - np.arange(10000)).all()
+
+
+def test_keymap_matches_reference_header():
+    with open(os.path.join(GOLD, "builtin_h_probe.json")) as f:
+        p = json.load(f)
+    bits = np.array([a for a, _ in p["f32"]], np.uint32)
+    got = O.keymap(bits.view(np.float32)).astype(np.uint64)
+    assert got.tolist() == [b for _, b in p["f32"]]
+    bits = np.array([int(a) for a, _ in p["f64"]], np.uint64)
+    assert O.keymap(bits.view(np.float64)).tolist() == [int(b) for _, b in p["f64"]]
+    for row in p["ints"]:
+        v = int(row[0])
+        assert O.keymap(np.array([v], np.int64).astype(np.int8))[0] == row[1]
+        assert O.keymap(np.array([v & 0xFF], np.uint8))[0] == row[2]
+        assert O.keymap(np.array([v], np.int64).astype(np.int16))[0] == row[3]
+        assert O.keymap(np.array([v & 0xFFFF], np.uint16))[0] == row[4]
+        assert O.keymap(np.array([v], np.int64).astype(np.int32))[0] == row[5]
+        assert O.keymap(np.array([v & 0xFFFFFFFF], np.uint32))[0] == row[6]
+        assert O.keymap(np.array([v], np.int64))[0] == int(row[7])
+        assert O.keymap(np.array([v % (1 << 64)], np.uint64))[0] == int(row[8])
+
+
+def test_maxmin_semantics_match_reference_header():
+    with open(os.path.join(GOLD, "builtin_h_probe.json")) as f:
+        p = json.load(f)
+    for xb, yb, mx, mn in p["maxmin_f32"]:
+        x, y = np.array([xb, yb], np.uint32).view(np.float32)
+        # Maximum: x < y ? y : x ; Minimum: x > y ? y : x (built_in.h:23-39)
+        a = y if x < y else x
+        b = y if x > y else x
+        assert np.array([a], np.float32).view(np.uint32)[0] == mx
+        assert np.array([b], np.float32).view(np.uint32)[0] == mn
+        # the oracle's scans/reductions use the same rule
+        assert O.reduce(np.array([y], np.float32), x, "Maximum").view(np.uint32) == mx
+
+
+@pytest.mark.parametrize("dt", [np.int8, np.uint8, np.int16, np.int32, np.uint32, np.int64, np.uint64,
+                                np.float32, np.float64])
+def test_fast_sort_equals_literal_bitsplit(dt):
+    rng = np.random.default_rng(0)
+    for n in (1, 2, 17, 300, 2000):
+        if np.issubdtype(dt, np.floating):
+            x = rng.standard_normal(n).astype(dt)
+            x[rng.integers(0, n, max(1, n // 20))] = np.nan
+            x[rng.integers(0, n, max(1, n // 20))] = -0.0
+            if n > 3:
+                x[0] = np.nan
+        else:
+            info = np.iinfo(dt)
+            x = rng.integers(info.min, info.max, n, dtype=dt, endpoint=True)
+        for desc in (False, True):
+            assert (O.sort_perm(x, desc) == O.sort_perm(x, desc, literal=True)).all()
+
+
+def test_min_element_tree_nan_selection():
+    # a NaN in a left slot absorbs its subtree: [5, NaN, 3, 0] selects 3, not 0
+    x = np.array([5, np.nan, 3, 0], np.float32)
+    assert O.min_element(x) == 2
+    # and the sorted output is the rotation that puts keys >= 3 first
+    assert O.sort(x).tolist()[:2] == [3.0, 5.0] and np.isnan(O.sort(x)[2]) and O.sort(x)[3] == 0.0
+
+
+def test_compaction_restatements():
+    x = np.array([1, 3, 3, 3, 2, 2, 1], np.int32)
+    assert x[O.unique_flags(x)].tolist() == [1, 3, 2, 1]
+    assert x[O.remove_flags(x, 3)].tolist() == [1, 2, 2, 1]
+    out, c = O.partition(np.arange(1, 11), np.arange(1, 11) % 2 == 0)
+    assert out.tolist() == [2, 4, 6, 8, 10, 1, 3, 5, 7, 9] and c == 5
+    k, v = O.reduce_by_key(x, np.array([9, 8, 7, 6, 5, 4, 3], np.int32))
+    assert k.tolist() == [1, 3, 2, 1] and v.tolist() == [9, 21, 9, 3]

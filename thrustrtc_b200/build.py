@@ -27,7 +27,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-re
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True) + \
+    return glob.glob(os.path.join(INCLUDE, "*.h")) + glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True) + \
         glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True)
 
 
@@ -57,8 +57,11 @@ def _embed_headers():
     return path
 
 
+INCLUDE = os.path.join(os.path.dirname(PKG), "include")
+
+
 def _compile(src, obj):
-    cmd = [NVCC] + ARCH + FLAGS + ["-I", CSRC, "-c", src, "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + ["-I", CSRC, "-I", INCLUDE, "-I", os.path.join(CSRC, "host"), "-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("compile failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))

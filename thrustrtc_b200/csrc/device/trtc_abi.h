@@ -6,12 +6,13 @@
 namespace trtc {
 
 struct LookbackState {
-    unsigned int* flags;            // [tiles] epoch4 + 1 (aggregate) / epoch4 + 2 (inclusive)
-    void* agg;                      // [tiles] tile aggregates (value type of the scan)
-    void* incl;                     // [tiles] inclusive prefixes
-    unsigned char* heads;           // [tiles] segmented scans: tile contains a segment head
+    unsigned int* flags;            // [tiles] flag word: epoch8 + state (1 aggregate, 2 inclusive)
+                                    //         + 4 when the tile holds a segment head
+    unsigned long long* packed;     // [tiles] values of <= 4 bytes: (flag word << 32) | value bits
+    void* agg;                      // [tiles] aggregates of larger values
+    void* incl;                     // [tiles] inclusive prefixes of larger values
     unsigned long long* tile_ctr;   // tile ticket counter (zero between launches)
-    unsigned int epoch4;
+    unsigned int epoch8;            // per-launch epoch * 8: stale flags never look valid
     unsigned int* err;              // host-visible error word
     void* result;                   // optional: the last tile stores the grand total here
 };

@@ -61,10 +61,26 @@ TRTC_FORCEINLINE void st_release(uint32_t* p, uint32_t v) {
 TRTC_FORCEINLINE void st_release(unsigned long long* p, unsigned long long v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+// Polls use relaxed loads (independent polls may be in flight together; an acquire load
+// would order every later load behind it) followed by one fence before the values that the
+// flags publish are read.
 TRTC_FORCEINLINE uint32_t ld_relaxed(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
+}
+TRTC_FORCEINLINE unsigned long long ld_relaxed(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+TRTC_FORCEINLINE void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// Stores of status words that carry their own value: no ordering with other data needed.
+TRTC_FORCEINLINE void st_relaxed(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+TRTC_FORCEINLINE void st_relaxed(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 TRTC_FORCEINLINE uint32_t lane_id() { return threadIdx.x & 31u; }

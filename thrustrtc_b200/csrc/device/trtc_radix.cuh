@@ -14,7 +14,7 @@
 //     internal/general_reduce.cpp:55-95) can select a non-minimum when NaNs sit in left slots;
 //     the sorted order is then a rotation, applied by the last digit pass's scatter;
 //   * one pass kernel per digit: a CTA takes tiles in launch order from an atomic counter,
-//     ranks its keys with warp multisplit (__match_any_sync), publishes per-digit counts,
+//     ranks its keys with warp multisplit (bit ballots), publishes per-digit counts,
 //     looks back across earlier tiles for its global offsets (decoupled look-back with
 //     release/acquire flags and bounded spins), stages the tile in shared memory in digit
 //     order and writes it out in bucket runs.
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(BLOCK) radix_count_below_kernel(const typename
 // HAS_VALS: move a 4- or 8-byte payload with the keys.  vals_from_index: the payload of the
 // first active pass is the element index (used to sort a permutation for odd value sizes).
 template <class K, class V, bool HAS_VALS, bool DESC, int BLOCK, int ITEMS, class ST>
-__global__ void __launch_bounds__(BLOCK) radix_pass_kernel(SortBufs bufs, size_t n, SortCtrl* ctrl, int pass,
+__global__ void __launch_bounds__(BLOCK, (ITEMS >= 24 ? 2 : 3)) radix_pass_kernel(SortBufs bufs, size_t n, SortCtrl* ctrl, int pass,
                                                            ST* status0, ST* status1, int vals_from_index) {
     static_assert(BLOCK >= 256, "one thread per digit is needed");
     constexpr int TILE = BLOCK * ITEMS;
@@ -312,37 +312,51 @@ __global__ void __launch_bounds__(BLOCK) radix_pass_kernel(SortBufs bufs, size_t
     const bool full = tile_base + TILE <= n;
 
     KB keys[ITEMS];
-    V vals[HAS_VALS ? ITEMS : 1];
     uint32_t rank[ITEMS];
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
         const size_t idx = wbase + (size_t)i * 32 + lane;
-        if (full || idx < n) {
-            keys[i] = src_k[idx];
-            if (HAS_VALS) vals[i] = index_payload ? (V)idx : src_v[idx];
-        } else {
-            keys[i] = KB(0);
-            if (HAS_VALS) vals[i] = V();
-        }
+        keys[i] = (full || idx < n) ? src_k[idx] : KB(0);
     }
 
-    // warp multisplit ranking: stable within the warp (items in order, lanes in order)
+    // Warp multisplit ranking, stable within the warp (items in order, lanes in order).
+    // Per item: peers of the same digit (__match_any_sync), rank among them, and one
+    // shared-memory atomicAdd by the group leader that returns the warp's running count of
+    // that digit.  The atomics of successive items are independent instructions executed in
+    // issue order, so the items pipeline instead of forming a load->store chain.
     uint32_t* wh = s_whist + warp * 256;
     const uint32_t ltm = lanemask_lt();
+    uint32_t info[ITEMS];  // rank among peers | leader lane << 8
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
         const size_t idx = wbase + (size_t)i * 32 + lane;
         const uint32_t d = (full || idx < n) ? radix_digit<K, DESC>(keys[i], shift) : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const int leader = __ffs(peers) - 1;
-        uint32_t before = 0;
-        if (lane == leader && d < 256u) {
-            before = wh[d];
-            wh[d] = before + (uint32_t)__popc(peers);
+        // peers with the same digit: AND of 9 bit-ballots (cheaper than __match_any_sync on
+        // sm_100; the 9th bit separates the out-of-range slots of a partial tile)
+        uint32_t peers = 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < 9; b++) {
+            const uint32_t bit = (d >> b) & 1u;
+            const uint32_t bb = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? bb : ~bb;
         }
-        before = __shfl_sync(0xffffffffu, before, leader);
-        rank[i] = before + (uint32_t)__popc(peers & ltm);
-        __syncwarp();
+        const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+        info[i] = (uint32_t)__popc(peers & ltm) | (leader << 8);
+        rank[i] = 0;
+        if (lane == leader && d < 256u) rank[i] = atomicAdd(&wh[d], (uint32_t)__popc(peers));
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+        rank[i] = __shfl_sync(0xffffffffu, rank[i], (int)(info[i] >> 8)) + (info[i] & 0xFFu);
+
+    // payloads are loaded only now (their registers were not needed during ranking)
+    V vals[HAS_VALS ? ITEMS : 1];
+    if (HAS_VALS) {
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const size_t idx = wbase + (size_t)i * 32 + lane;
+            vals[i] = (full || idx < n) ? (index_payload ? (V)idx : src_v[idx]) : V();
+        }
     }
     __syncthreads();
 
@@ -360,7 +374,7 @@ __global__ void __launch_bounds__(BLOCK) radix_pass_kernel(SortBufs bufs, size_t
         cnt = sum;
         s_count[d] = sum;
         const ST flag = (ST)(tile == 0 ? 2u : 1u) << SB::SHIFT;
-        st_release(&st[tile * 256 + d], flag | (ST)sum);
+        st_relaxed(&st[tile * 256 + d], flag | (ST)sum);
     }
     const uint32_t start = block_excl_scan_256<BLOCK>(cnt, s_wsum);
     if (threadIdx.x < 256) s_start[threadIdx.x] = start;
@@ -378,25 +392,39 @@ __global__ void __launch_bounds__(BLOCK) radix_pass_kernel(SortBufs bufs, size_t
         }
     }
 
-    // decoupled look-back, one thread per digit
+    // decoupled look-back, one thread per digit.  Each round trip polls LB predecessor tiles
+    // at once (independent loads), so the inclusive-prefix frontier advances LB tiles per
+    // memory round trip instead of one.
     if (threadIdx.x < 256) {
+        constexpr int LB = 16;
         const int d = threadIdx.x;
         ST excl = 0;
         if (tile > 0) {
-            size_t j = tile - 1;
+            long long j = (long long)tile - 1;  // newest tile not yet accumulated
             uint32_t spins = 0;
-            while (true) {
-                const ST s = ld_acquire(&st[j * 256 + d]);
-                const uint32_t f = (uint32_t)(s >> SB::SHIFT);
-                if (f == 0) {
-                    if (!spin_continue(spins, bufs.err)) { report_error(bufs.err, TRTC_ERR_LOOKBACK_TIMEOUT); break; }
-                    continue;
+            bool done = false;
+            while (!done) {
+                ST s[LB];
+#pragma unroll
+                for (int k = 0; k < LB; k++)
+                    s[k] = (j - k >= 0) ? ld_relaxed(&st[(size_t)(j - k) * 256 + d]) : ((ST)2u << SB::SHIFT);
+                int used = 0;
+#pragma unroll
+                for (int k = 0; k < LB; k++) {
+                    if (done || used != k) continue;  // stop at the first tile not yet published
+                    const uint32_t f = (uint32_t)(s[k] >> SB::SHIFT);
+                    if (f == 0) continue;
+                    excl += s[k] & SB::MASK;
+                    used = k + 1;
+                    if (f == 2) done = true;
                 }
-                excl += s & SB::MASK;
-                if (f == 2 || j == 0) break;
-                --j;
+                j -= used;
+                if (!done && j < 0) done = true;
+                if (!done && used == 0) {
+                    if (!spin_continue(spins, bufs.err)) { report_error(bufs.err, TRTC_ERR_LOOKBACK_TIMEOUT); break; }
+                }
             }
-            st_release(&st[tile * 256 + d], ((ST)2u << SB::SHIFT) | (excl + (ST)s_count[d]));
+            st_relaxed(&st[tile * 256 + d], ((ST)2u << SB::SHIFT) | (excl + (ST)s_count[d]));
         }
         s_adj[d] = plan.base[pass][d] + (uint32_t)excl - s_start[d];
     }

@@ -51,64 +51,123 @@ TRTC_FORCEINLINE void opt_combine(T& a, bool& ah, const T& b, bool bh, Op& op) {
 // Returns the ordered combination of all tiles before `tile` (their values being inclusive
 // prefixes or aggregates).  SEG: stop at the first tile holding a segment head as well, and
 // combine with the segmented operator (a head in the right operand discards the left).
+//
+// One round trip polls TRTC_LB_K blocks of 32 consecutive predecessor tiles (coalesced
+// relaxed loads, all in flight together): the inclusive frontier must advance as fast as
+// tiles start on 148 SMs.  Values of <= 4 bytes travel in the same 64-bit word as their
+// flag (no fence, no second load); larger values are read after one acquire fence.
+#ifndef TRTC_LB_K
+#define TRTC_LB_K 4
+#endif
+template <class T> struct LbPack { static constexpr bool value = sizeof(T) <= 4; };
+
+template <class T>
+TRTC_FORCEINLINE uint32_t lb_bits(const T& v) {
+    union U { T t; uint32_t u; TRTC_FORCEINLINE U() : u(0) {} } c;
+    c.t = v;
+    return c.u;
+}
+template <class T>
+TRTC_FORCEINLINE T lb_value(uint32_t u) {
+    union U { T t; uint32_t u; TRTC_FORCEINLINE U() : u(0) {} } c;
+    c.u = u;
+    return c.t;
+}
+TRTC_FORCEINLINE uint32_t lb_state(uint32_t fw, uint32_t epoch8) {
+    const uint32_t r = fw - epoch8;  // valid words: 1, 2, 5, 6
+    return (fw >= epoch8 && r < 8u && (r & 3u) != 0u && (r & 3u) != 3u) ? r : 0u;
+}
+
 template <class T, class Op, bool SEG>
 __device__ inline Opt<T> lookback_prefix(const LookbackState& st, size_t tile, Op& op, bool& seg_flag_out) {
+    constexpr int K = TRTC_LB_K;
+    constexpr bool PACK = LbPack<T>::value;
     const uint32_t lane = lane_id();
-    const T* agg = reinterpret_cast<const T*>(st.agg);
-    const T* inc = reinterpret_cast<const T*>(st.incl);
     T acc = T();
-    bool has = false, acc_head = false;
-    long long j0 = (long long)tile - 1;
-    while (j0 >= 0) {
-        const long long j = j0 - (long long)lane;
-        uint32_t state = 3;  // beyond tile 0: acts as a stop with no value
-        if (j >= 0) {
-            uint32_t spins = 0;
-            while (true) {
-                const uint32_t raw = ld_acquire(&st.flags[j]);
-                if (raw >= st.epoch4 + 1u && raw <= st.epoch4 + 2u) { state = raw - st.epoch4; break; }
-                if (!spin_continue(spins, st.err)) { report_error(st.err, TRTC_ERR_LOOKBACK_TIMEOUT); state = 2; break; }
-            }
-        }
-        T v = T();
-        bool hd = false;
-        if (j >= 0) {
-            v = (state == 2) ? inc[j] : agg[j];
-            if (SEG) hd = st.heads[j] != 0;
-        }
-        const uint32_t stop_mask = __ballot_sync(0xffffffffu, state >= 2u || (SEG && hd));
-        const int stop = stop_mask ? __ffs(stop_mask) - 1 : 31;
-        bool vh = (int)lane <= stop && j >= 0;
-        // ordered tree: lane l combines with lane l+d (older => left operand)
+    bool has = false, acc_head = false, done = false;
+    long long j0 = (long long)tile - 1;  // newest tile not yet combined
+    while (!done && j0 >= 0) {
+        // ---- poll K blocks of 32 tiles: lane l of block k holds tile j0 - 32k - l
+        uint32_t code[K];
+        T val[K];
+        uint32_t spins = 0;
+        while (true) {
+            bool ready = true;
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const T o = shfl_down_any(v, d);
-            const int oh_i = __shfl_down_sync(0xffffffffu, (int)vh, d);
-            const int ohd = __shfl_down_sync(0xffffffffu, (int)hd, d);
-            const bool oh = oh_i && ((int)lane + d < 32);
-            if ((lane & (2 * d - 1)) == 0 && oh) {
-                if (SEG) {
-                    // o (older) ⊕ v (newer): a head in v keeps v
-                    if (!vh) { v = o; hd = ohd; }
-                    else if (!hd) { v = (T)op(o, v); hd = ohd; }
-                } else {
-                    v = vh ? (T)op(o, v) : o;
+            for (int k = 0; k < K; k++) {
+                const long long j = j0 - 32ll * k - (long long)lane;
+                code[k] = 8u;  // beyond tile 0
+                if (j >= 0) {
+                    if constexpr (PACK) {
+                        const unsigned long long w = ld_relaxed(&st.packed[j]);
+                        code[k] = lb_state((uint32_t)(w >> 32), st.epoch8);
+                        val[k] = lb_value<T>((uint32_t)w);
+                    } else {
+                        code[k] = lb_state(ld_relaxed(&st.flags[j]), st.epoch8);
+                    }
+                    ready = ready && code[k] != 0u;
                 }
-                vh = true;
+            }
+            if (__all_sync(0xffffffffu, ready)) break;
+            if (!spin_continue(spins, st.err)) {
+                report_error(st.err, TRTC_ERR_LOOKBACK_TIMEOUT);
+#pragma unroll
+                for (int k = 0; k < K; k++) if (code[k] == 0u) code[k] = 2u;
+                break;
             }
         }
-        // window total sits in lane 0; it is older than what was accumulated so far
-        if (vh && lane == 0) {
-            if (SEG) {
-                if (!has) { acc = v; acc_head = hd; }
-                else if (!acc_head) { acc = (T)op(v, acc); acc_head = hd; }
-            } else {
-                acc = has ? (T)op(v, acc) : v;
+        if constexpr (!PACK) {
+            fence_acq_rel();  // values are read after their flags
+            const T* agg = reinterpret_cast<const T*>(st.agg);
+            const T* inc = reinterpret_cast<const T*>(st.incl);
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const long long j = j0 - 32ll * k - (long long)lane;
+                val[k] = T();
+                if (j >= 0) val[k] = ((code[k] & 3u) == 2u) ? inc[j] : agg[j];
             }
-            has = true;
         }
-        if (stop_mask) break;
-        j0 -= 32;
+        // ---- combine block by block, newest first (older values are left operands)
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (done) continue;
+            const uint32_t c = code[k];
+            const bool beyond = c == 8u;
+            const bool hd0 = SEG && !beyond && (c & 4u);
+            const bool stop_here = beyond || (c & 3u) == 2u || hd0;
+            const uint32_t stop_mask = __ballot_sync(0xffffffffu, stop_here);
+            const int stop = stop_mask ? __ffs(stop_mask) - 1 : 31;
+            T v = val[k];
+            bool vh = (int)lane <= stop && !beyond;
+            bool hd = hd0;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const T o = shfl_down_any(v, d);
+                const int oh_i = __shfl_down_sync(0xffffffffu, (int)vh, d);
+                const int ohd = __shfl_down_sync(0xffffffffu, (int)hd, d);
+                const bool oh = oh_i && ((int)lane + d < 32);
+                if ((lane & (2 * d - 1)) == 0 && oh) {
+                    if (SEG) {
+                        if (!vh) { v = o; hd = ohd; }
+                        else if (!hd) { v = (T)op(o, v); hd = ohd; }
+                    } else {
+                        v = vh ? (T)op(o, v) : o;
+                    }
+                    vh = true;
+                }
+            }
+            if (vh && lane == 0) {
+                if (SEG) {
+                    if (!has) { acc = v; acc_head = hd; }
+                    else if (!acc_head) { acc = (T)op(v, acc); acc_head = hd; }
+                } else {
+                    acc = has ? (T)op(v, acc) : v;
+                }
+                has = true;
+            }
+            if (stop_mask) done = true;
+        }
+        j0 -= 32ll * K;
     }
     Opt<T> r;
     r.v = shfl_any(acc, 0);
@@ -119,10 +178,16 @@ __device__ inline Opt<T> lookback_prefix(const LookbackState& st, size_t tile, O
 
 template <class T>
 TRTC_FORCEINLINE void publish(const LookbackState& st, size_t tile, const T& v, bool inclusive, bool head) {
-    T* dst = reinterpret_cast<T*>(inclusive ? st.incl : st.agg);
-    dst[tile] = v;
-    if (st.heads) st.heads[tile] = head ? 1 : 0;
-    st_release(&st.flags[tile], st.epoch4 + (inclusive ? 2u : 1u));
+    const uint32_t fw = st.epoch8 + (inclusive ? 2u : 1u) + (head ? 4u : 0u);
+    if constexpr (LbPack<T>::value) {
+        // flag and value in one single-copy-atomic 64-bit store
+        const unsigned long long w = ((unsigned long long)fw << 32) | (unsigned long long)lb_bits<T>(v);
+        asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(&st.packed[tile]), "l"(w) : "memory");
+    } else {
+        T* dst = reinterpret_cast<T*>(inclusive ? st.incl : st.agg);
+        dst[tile] = v;
+        st_release(&st.flags[tile], fw);
+    }
 }
 
 TRTC_FORCEINLINE size_t claim_tile(const LookbackState& st, uint32_t* s_slot) {
@@ -144,7 +209,7 @@ TRTC_FORCEINLINE size_t claim_tile(const LookbackState& st, uint32_t* s_slot) {
 // l*VEC + e: a warp reads 32 consecutive 16-byte vectors per chunk (coalesced), and each
 // lane owns VEC consecutive elements, folded in registers before the warp-level scan.
 // MODE 0: inclusive.  MODE 1: exclusive with init (out[0] = init).  MODE 2: reduction only
-// (no output; the last tile stores the total in st.result).
+// (no output; the last tile stores the total in st.result).  MODE 3: reduction of init, x0, x1, ...
 template <class InV, class UOp, bool HAS_UOP, class OutV, class T, class Op, int MODE, int BLOCK, int NV>
 __global__ void __launch_bounds__(BLOCK) scan_kernel(InV in, UOp uop, OutV out, size_t n, Op op, T init,
                                                      LookbackState st) {
@@ -245,13 +310,13 @@ __global__ void __launch_bounds__(BLOCK) scan_kernel(InV in, UOp uop, OutV out, 
         T tp = T();
         bool tp_h = false;
         if (tile == 0) {
-            if (MODE == 1) { tp = init; tp_h = true; }
+            if (MODE == 1 || MODE == 3) { tp = init; tp_h = true; }
             T incl = tp;
             bool incl_h = tp_h;
             opt_combine(incl, incl_h, agg, agg_h, op);
             if (lane == 0) {
                 publish<T>(st, 0, incl, true, false);
-                if (MODE == 2 && valid == n && st.result) *reinterpret_cast<T*>(st.result) = incl;
+                if (MODE >= 2 && valid == n && st.result) *reinterpret_cast<T*>(st.result) = incl;
             }
         } else {
             if (lane == 0) publish<T>(st, tile, agg, false, false);
@@ -264,12 +329,12 @@ __global__ void __launch_bounds__(BLOCK) scan_kernel(InV in, UOp uop, OutV out, 
             opt_combine(incl, incl_h, agg, agg_h, op);
             if (lane == 0) {
                 publish<T>(st, tile, incl, true, false);
-                if (MODE == 2 && tile_base + valid == n && st.result) *reinterpret_cast<T*>(st.result) = incl;
+                if (MODE >= 2 && tile_base + valid == n && st.result) *reinterpret_cast<T*>(st.result) = incl;
             }
         }
         if (lane == 0) { s_pre = tp; s_pre_has = tp_h ? 1 : 0; }
     }
-    if (MODE == 2) return;
+    if (MODE >= 2) return;
     __syncthreads();
 
     // warp prefix = tile prefix ⊕ aggregates of earlier warps

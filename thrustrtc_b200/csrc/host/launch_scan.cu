@@ -19,9 +19,9 @@ static bool fill_lookback(LookbackState& st, cudaStream_t s, size_t tiles, size_
     st.flags = w->flags;
     st.agg = w->agg;
     st.incl = w->incl;
-    st.heads = seg ? w->heads : nullptr;
+    st.packed = w->packed;
     st.tile_ctr = w->tile_ctr;
-    st.epoch4 = e4;
+    st.epoch8 = e4;
     st.err = device_error_word();
     st.result = w->result;
     return true;

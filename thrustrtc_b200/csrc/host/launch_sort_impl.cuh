@@ -7,6 +7,7 @@
 
 namespace trtc_host {
 
+// items per thread of a digit pass (tile = 256 * ITEMS keys), from a sweep on B200 at 2^28 keys
 template <class K> struct SortTuning { enum { ITEMS = sizeof(K) >= 8 ? 8 : 16 }; };
 
 // Opts a kernel in to `bytes` of dynamic shared memory (needed as soon as static +
@@ -25,11 +26,10 @@ static void set_smem_attr_once(F* kernel, size_t bytes) {
 
 // Runs the whole sort on stream s.  vals0 may be null (keys only).  vals_from_index: the
 // payload is the element index (vals0 then receives the sorting permutation).
-template <class K, class V, bool HAS_VALS, bool DESC, class ST>
+template <class K, class V, bool HAS_VALS, bool DESC, class ST, int ITEMS = SortTuning<K>::ITEMS>
 static bool radix_sort_run(K* keys, V* vals0, size_t n, cudaStream_t s, int vals_from_index) {
     using namespace trtc;
     constexpr int BLOCK = 256;
-    constexpr int ITEMS = SortTuning<K>::ITEMS;
     constexpr int TILE = BLOCK * ITEMS;
     constexpr int D = RadixKey<K>::DIGITS;
     constexpr bool FLOATKEY = is_same<K, float>::value || is_same<K, double>::value;

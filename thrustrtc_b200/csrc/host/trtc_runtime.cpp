@@ -109,21 +109,21 @@ static LookbackWs* ws_for(cudaStream_t s) {
     return w;
 }
 
-LookbackWs* lookback_ws(cudaStream_t s, size_t tiles, size_t value_size, uint32_t* epoch4) {
+LookbackWs* lookback_ws(cudaStream_t s, size_t tiles, size_t value_size, uint32_t* epoch8) {
     std::lock_guard<std::mutex> lk(g_mu);
     LookbackWs* w = ws_for(s);
     if (value_size < 8) value_size = 8;
     const bool grow = tiles > w->tiles_cap || value_size > w->value_cap;
-    if (grow || w->epoch >= (1u << 29)) {
+    if (grow || w->epoch >= (1u << 28)) {
         // the old arrays may still be in use by queued work on this stream
         cudaStreamSynchronize(s);
         if (grow) {
             size_t cap = tiles > w->tiles_cap ? tiles : w->tiles_cap;
             if (cap < 1024) cap = 1024;
             size_t vcap = value_size > w->value_cap ? value_size : w->value_cap;
-            cudaFree(w->flags); cudaFree(w->agg); cudaFree(w->incl); cudaFree(w->heads);
+            cudaFree(w->flags); cudaFree(w->agg); cudaFree(w->incl); cudaFree(w->packed);
             if (!TRTC_CUDA(cudaMalloc(&w->flags, cap * 4)) || !TRTC_CUDA(cudaMalloc(&w->agg, cap * vcap)) ||
-                !TRTC_CUDA(cudaMalloc(&w->incl, cap * vcap)) || !TRTC_CUDA(cudaMalloc(&w->heads, cap))) {
+                !TRTC_CUDA(cudaMalloc(&w->incl, cap * vcap)) || !TRTC_CUDA(cudaMalloc(&w->packed, cap * 8))) {
                 w->tiles_cap = 0;
                 return nullptr;
             }
@@ -134,12 +134,13 @@ LookbackWs* lookback_ws(cudaStream_t s, size_t tiles, size_t value_size, uint32_
             if (!TRTC_CUDA(cudaMalloc(&w->tile_ctr, 16)) || !TRTC_CUDA(cudaMalloc(&w->result, 16))) return nullptr;
         }
         cudaMemset(w->flags, 0, w->tiles_cap * 4);
+        cudaMemset(w->packed, 0, w->tiles_cap * 8);
         cudaMemset(w->tile_ctr, 0, 16);
         cudaDeviceSynchronize();
         w->epoch = 0;
     }
     w->epoch += 1;
-    *epoch4 = w->epoch * 4u;
+    *epoch8 = w->epoch * 8u;
     return w;
 }
 

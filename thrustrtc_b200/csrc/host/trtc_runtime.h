@@ -36,7 +36,7 @@ struct LookbackWs {
     uint32_t* flags = nullptr;
     void* agg = nullptr;
     void* incl = nullptr;
-    unsigned char* heads = nullptr;
+    unsigned long long* packed = nullptr;  // flag + value words for values of <= 4 bytes
     unsigned long long* tile_ctr = nullptr;
     unsigned long long* result = nullptr;  // device scalar (count / total)
     size_t tiles_cap = 0;
@@ -52,7 +52,7 @@ struct LookbackWs {
 };
 // Reserves room for `tiles` tiles of `value_size`-byte values; returns the workspace with
 // its flag epoch advanced for one launch.
-LookbackWs* lookback_ws(cudaStream_t s, size_t tiles, size_t value_size, uint32_t* epoch4);
+LookbackWs* lookback_ws(cudaStream_t s, size_t tiles, size_t value_size, uint32_t* epoch8);
 LookbackWs* reduce_ws(cudaStream_t s, size_t partials, size_t value_size);
 void* sort_ctrl_ws(cudaStream_t s, size_t bytes);
 
