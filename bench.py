@@ -1,0 +1,515 @@
+#!/usr/bin/env python
+"""Benchmark of the thrustrtc_b200 hot path on B200.
+
+Default workload: stable Sort_By_Key of 2^28 uint32 keys (uniform over the 32-bit range,
+SplitMix64 seed 0) with uint32 values = index, ascending -- the reference's headline case.
+Other workloads (--workload): inclusive scan of 2^28 int32 in [-1000, 1000], reduce of 2^28
+float32 in [0, 1).
+
+One JSON line on rank 0:
+  value        whole-job throughput with inputs resident in HBM (device-timed with CUDA
+               events on the launching stream; max over ranks)
+  e2e          the same metric through the drop-in C ABI (n_dvvector_create from pinned host
+               memory, n_sort_by_key / n_inclusive_scan / n_reduce, n_dvvector_to_host)
+  roofline     the dominant kernel's algorithmic bytes per launch / its average device time
+               (per-launch CUDA events recorded by the library over the timed region)
+  cpu_baseline the oracle's host sort / scan / reduce on a bounded sample, all host threads
+
+`--impl reference` times the reference algorithm's CPU restatement (the reference itself has
+no CPU path and does not build here) on the same workload definition.
+
+Multi-GPU (torchrun, one process per GPU): every rank runs the same workload on its own GPU
+(replicas, weak scaling); there is no collective on the data path.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+L2_BYTES = 126 * 1024 * 1024
+
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant kernel,
+# per unit processed (bytes per pair / element); None until a capture of the current kernel
+# exists.  Source summaries: profiles/<kernel>_<workload>.md
+NCU_TRAFFIC_PER_UNIT = {
+    "sort_by_key_u32": None,
+    "inclusive_scan_i32": None,
+    "reduce_f32": None,
+}
+
+WORKLOADS = {
+    # name: (default n, dominant kernel, algorithmic bytes per unit per dominant launch,
+    #        algorithmic bytes per unit for the whole operation, metric, unit)
+    "sort_by_key_u32": (1 << 28, "radix_pass_kernel", 16, 68,
+                        "Gkeys/s sort 2^28 u32 pairs, % HBM roofline", "Gkeys/s"),
+    "inclusive_scan_i32": (1 << 28, "scan_kernel", 8, 8, "GB/s inclusive scan 2^28 i32, % HBM roofline", "GB/s"),
+    "reduce_f32": (1 << 28, "reduce_kernel", 4, 4, "GB/s reduce 2^28 f32, % HBM roofline", "GB/s"),
+}
+
+M64 = (1 << 64) - 1
+GAMMA = 0x9E3779B97F4A7C15
+
+
+def _mix64(z):
+    """SplitMix64 output function (Steele, Lea & Flood 2014) on a numpy uint64 array."""
+    z = z ^ (z >> np.uint64(30))
+    z = z * np.uint64(0xBF58476D1CE4E5B9)
+    z = z ^ (z >> np.uint64(27))
+    z = z * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def splitmix64(seed, stream, n, start=0, chunk=1 << 24):
+    """Counter-based SplitMix64: element i is the (i+1)-th output of SplitMix64 started at
+    state base = mix(seed << 8 | stream), i.e. mix(base + (i + 1) * GAMMA)."""
+    base = int(_mix64(np.array([((seed << 8) | stream) & M64], np.uint64))[0])
+    out = np.empty(n, np.uint64)
+    with np.errstate(over="ignore"):
+        for a in range(0, n, chunk):
+            b = min(n, a + chunk)
+            i = np.arange(start + a + 1, start + b + 1, dtype=np.uint64)
+            out[a:b] = _mix64(np.uint64(base) + i * np.uint64(GAMMA))
+    return out
+
+
+def gen_inputs(workload, n):
+    """Host inputs of a workload (identical bytes for the GPU runs, the oracle and the
+    reference arm)."""
+    if workload == "sort_by_key_u32":
+        keys = (splitmix64(0, 0, n) >> np.uint64(32)).astype(np.uint32)
+        vals = np.arange(n, dtype=np.uint32)
+        return keys, vals
+    if workload == "inclusive_scan_i32":
+        h = splitmix64(0, 0, n)
+        return ((h % np.uint64(2001)).astype(np.int64) - 1000).astype(np.int32), None
+    if workload == "reduce_f32":
+        h = splitmix64(0, 0, n)
+        return ((h >> np.uint64(40)).astype(np.float64) * 2.0 ** -24).astype(np.float32), None
+    raise ValueError(workload)
+
+
+# ---------------------------------------------------------------- clocks during the timed region
+_REASONS = [(0x4, "sw_power_cap"), (0x8, "hw_slowdown"), (0x20, "sw_thermal_slowdown"),
+            (0x40, "hw_thermal_slowdown"), (0x80, "hw_power_brake_slowdown"), (0x2, "applications_clocks_setting"),
+            (0x10, "sync_boost"), (0x100, "display_clock_setting")]
+
+
+class ClockSampler:
+    """Reads SM clock and clock-event reasons through NVML every `period` s (read-only)."""
+
+    def __init__(self, torch_dev, period=0.01):
+        self.samples, self.reasons, self.ok = [], set(), False
+        self.period = period
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            import torch
+            p = torch.cuda.get_device_properties(torch_dev)
+            bus = "%08x:%02x:%02x.0" % (getattr(p, "pci_domain_id", 0), p.pci_bus_id, p.pci_device_id)
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception as e:  # noqa: BLE001  (no NVML: report clocks as unavailable)
+            self.err = str(e)
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in _REASONS:
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self._stop = threading.Event()
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "note": "NVML unavailable"}
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "of measured"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "of fallback"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def cpu_threads():
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_run(workload, sample_n, threads):
+    """One timed oracle run on the host over the first `sample_n` units; returns (seconds,
+    threads used): the pair sort runs on `threads` threads, the scan and reduce on one."""
+    from oracle import oracle as O
+    x, v = gen_inputs(workload, sample_n)
+    t0 = time.perf_counter()
+    if workload == "sort_by_key_u32":
+        O.sort_pairs32(x, v, False, threads)
+    elif workload == "inclusive_scan_i32":
+        O.scan(x)
+    else:
+        O.reduce(x)
+    return time.perf_counter() - t0, (threads if workload == "sort_by_key_u32" else 1)
+
+
+def units_per_s_to_metric(workload, units, seconds):
+    """Throughput in the metric's unit: Gkeys/s for sorts, GB/s of algorithmic bytes otherwise."""
+    if workload == "sort_by_key_u32":
+        return units / seconds / 1e9
+    return units * WORKLOADS[workload][3] / seconds / 1e9
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    wl = args.workload
+    n, _, _, _, metric, unit = WORKLOADS[wl]
+    threads = cpu_threads()
+    sample = args.cpu_sample or (1 << 25 if wl == "sort_by_key_u32" else 1 << 27)
+    from oracle import oracle as O
+    O.build()
+    for _ in range(args.warmup):
+        cpu_run(wl, sample, threads)
+    ts = [cpu_run(wl, sample, threads) for _ in range(args.steps)]
+    tot = sum(t for t, _ in ts)
+    threads = ts[0][1]
+    value = units_per_s_to_metric(wl, sample * args.steps, tot)
+    desc = ("first %d units of the %s workload (n=%d); oracle restatement of the reference's "
+            "algorithm, %d host threads" % (sample, wl, n, threads))
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": _dtype(wl),
+            "data": "synthetic (SplitMix64 seed 0)", "config": _config(wl, n, world),
+            "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference (fynv/ThrustRTC) has no CPU path and does not build in this image; "
+                    "the arm times the oracle's host restatement of its algorithm"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _dtype(wl):
+    return {"sort_by_key_u32": "u32", "inclusive_scan_i32": "int32", "reduce_f32": "f32"}[wl]
+
+
+def _config(wl, n, world):
+    base = {"workload": wl, "n": n, "parallelism": "replicas x%d" % world,
+            "l2": "inputs (%d MiB) exceed the 126 MB L2" % (n * (8 if wl == "sort_by_key_u32" else 4) >> 20)}
+    if wl == "sort_by_key_u32":
+        base.update({"keys": "uint32 uniform over 32 bits", "values": "uint32 = index", "order": "ascending, stable",
+                     "step": "restore the unsorted pairs from a pristine copy (untimed), then one sort (timed)"})
+    elif wl == "inclusive_scan_i32":
+        base.update({"values": "int32 uniform in [-1000, 1000]", "op": "Plus"})
+    else:
+        base.update({"values": "float32 uniform in [0, 1)", "op": "Plus", "accumulation": "fp32"})
+    return base
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: a CUDA device is required (there is no CPU path)")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    import thrustrtc_b200 as trtc
+    from thrustrtc_b200 import _native as N
+    trtc.init()
+    L = N.lib
+    wl = args.workload
+    n, kname, b_launch, b_unit, metric, unit = WORKLOADS[wl]
+    n = args.n or n
+    assert args.warmup >= 3 or args.allow_short_warmup, "at least 3 warm-up steps"
+
+    keys_h, vals_h = gen_inputs(wl, n)
+    stream = None  # the legacy default stream: torch's current stream and the library's
+    if wl == "sort_by_key_u32":
+        k0 = torch.from_numpy(keys_h.view(np.int32)).to(dev)
+        v0 = torch.from_numpy(vals_h.view(np.int32)).to(dev)
+        k, v = torch.empty_like(k0), torch.empty_like(v0)
+
+        def restore():
+            k.copy_(k0)
+            v.copy_(v0)
+
+        def step():
+            if L.trtc_raw_sort_by_key(5, ctypes.c_void_p(k.data_ptr()), ctypes.c_void_p(v.data_ptr()), 4, n, 0,
+                                      stream) != 0:
+                raise RuntimeError(N.last_error())
+    elif wl == "inclusive_scan_i32":
+        x = torch.from_numpy(keys_h).to(dev)
+        y = torch.empty_like(x)
+        flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
+
+        def restore():
+            flush.fill_(1)  # evicts the previous step's lines from L2
+
+        def step():
+            if L.trtc_raw_scan(4, 0, 0, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()), n, None,
+                               stream) != 0:
+                raise RuntimeError(N.last_error())
+    else:
+        x = torch.from_numpy(keys_h).to(dev)
+        flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
+        res = ctypes.c_void_p()
+
+        def restore():
+            flush.fill_(1)
+
+        def step():
+            if L.trtc_raw_reduce_async(8, 0, ctypes.c_void_p(x.data_ptr()), n, None, ctypes.byref(res), stream) != 0:
+                raise RuntimeError(N.last_error())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        restore()
+        step()
+    barrier()
+
+    # ---- timed region: K steps, each bracketed by events on the launching stream
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(dev)
+    lc0 = N.launch_count()
+    N.timing_enable(True)
+    with sampler:
+        barrier()
+        for i in range(args.steps):
+            restore()
+            ev[i][0].record()
+            step()
+            ev[i][1].record()
+        barrier()
+    launches = N.launch_count() - lc0
+    recs = N.timing_records()
+    N.timing_enable(False)
+    if L.trtc_raw_sync(stream) != 0:
+        raise RuntimeError(N.last_error())
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    tot_ms = max_over_ranks(sum(step_ms))
+    value = units_per_s_to_metric(wl, n * world * args.steps, tot_ms / 1e3)
+
+    # ---- correctness of the last step (size-independent properties), loud on failure
+    _check(wl, n, locals())
+
+    # ---- dominant kernel roofline from the per-launch events of the timed region
+    kt = [ms for name, ms in recs if name == kname]
+    peak, peak_src = measured_peak()
+    per_launch_ms = statistics.mean(kt) if kt else None
+    achieved = (b_launch * n / (per_launch_ms / 1e3) / 1e9) if per_launch_ms else None
+    traffic = NCU_TRAFFIC_PER_UNIT.get(wl)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "peak_source": peak_src,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                "traffic": (traffic * n) if traffic else None, "algorithmic_bytes_per_launch": b_launch * n,
+                "launch_ms": per_launch_ms, "launches_timed": len(kt)}
+    whole = b_unit * n / (tot_ms / args.steps / 1e3) / 1e9
+    kernel_share = {}
+    for name, ms in recs:
+        kernel_share[name] = kernel_share.get(name, 0.0) + ms
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = _e2e(args, wl, n, keys_h, vals_h, world, max_over_ranks, barrier)
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu:
+        threads = cpu_threads()
+        sample = args.cpu_sample or (1 << 25 if wl == "sort_by_key_u32" else 1 << 27)
+        sample = min(sample, n)
+        secs, threads = cpu_run(wl, sample, threads)
+        cpu = {"value": units_per_s_to_metric(wl, sample, secs), "unit": unit, "cores": threads, "kind": "port",
+               "sample": "first %d units of the same workload, oracle host restatement, %d threads" % (sample, threads)}
+
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": _dtype(wl),
+                "data": "synthetic (SplitMix64 seed 0, generated on the host)", "config": _config(wl, n, world),
+                "roofline": roofline,
+                "roofline_whole_op": {"algorithmic_bytes_per_unit": b_unit, "achieved": whole,
+                                      "frac": whole / peak, "unit": "GB/s"},
+                "kernel_ms_timed_region": {k2: round(v2, 4) for k2, v2 in sorted(kernel_share.items())},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": sampler.summary(), "gpu_launches": launches,
+                "step_ms": [round(s, 4) for s in step_ms]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def _check(wl, n, env):
+    import torch
+    if wl == "sort_by_key_u32":
+        k, v, k0 = env["k"], env["v"], env["k0"]
+        ku = k.to(torch.int64) & 0xFFFFFFFF
+        if n > 1 and not bool((ku[1:] >= ku[:-1]).all()):
+            raise RuntimeError("sort check failed: keys not ascending")
+        perm = v.to(torch.int64)
+        if not bool((k0[perm] == k).all()):
+            raise RuntimeError("sort check failed: values are not the keys' permutation")
+        eq = ku[1:] == ku[:-1]
+        if n > 1 and not bool((perm[1:][eq] > perm[:-1][eq]).all()):
+            raise RuntimeError("sort check failed: not stable")
+        if int(torch.bincount(perm, minlength=n).max()) != 1:
+            raise RuntimeError("sort check failed: values are not a permutation")
+    elif wl == "inclusive_scan_i32":
+        x, y = env["x"], env["y"]
+        ref = torch.cumsum(x.to(torch.int64), 0)
+        if not bool((ref.to(torch.int32) == y).all()):
+            raise RuntimeError("scan check failed")
+    else:
+        x = env["x"]
+        import thrustrtc_b200._native as N
+        val = ctypes.c_float()
+        if N.lib.trtc_raw_reduce(8, 0, ctypes.c_void_p(x.data_ptr()), n, None, ctypes.byref(val), None) != 0:
+            raise RuntimeError(N.last_error())
+        ref = float(x.to(torch.float64).sum())
+        if abs(val.value - ref) > 1e-5 * abs(ref):
+            raise RuntimeError("reduce check failed: %r vs %r" % (val.value, ref))
+
+
+def _e2e(args, wl, n, keys_h, vals_h, world, max_over_ranks, barrier):
+    """Per step: H2D of the inputs from pinned host memory into new DVVectors, the call,
+    D2H of the result into pinned host memory, all through the n_* C ABI."""
+    import torch
+    from thrustrtc_b200.api import lib as A, check_i
+    kp = torch.from_numpy(keys_h.view(np.int32) if keys_h.dtype == np.uint32 else keys_h).pin_memory()
+    vp_ = torch.from_numpy(vals_h.view(np.int32)).pin_memory() if vals_h is not None else None
+    ko = torch.empty_like(kp).pin_memory()
+    vo = torch.empty_like(vp_).pin_memory() if vp_ is not None else None
+    esz = keys_h.dtype.itemsize
+    cls = {"sort_by_key_u32": b"uint32_t", "inclusive_scan_i32": b"int32_t", "reduce_f32": b"float"}[wl]
+    h2d = n * esz + (n * 4 if vp_ is not None else 0)
+    d2h = {"sort_by_key_u32": 2 * n * 4, "inclusive_scan_i32": n * 4, "reduce_f32": 4}[wl]
+    steps = max(1, min(args.steps, args.e2e_steps))
+
+    def one():
+        dk = A.n_dvvector_create(cls, n, ctypes.c_void_p(kp.data_ptr()))
+        if not dk:
+            raise RuntimeError("n_dvvector_create failed")
+        try:
+            if wl == "sort_by_key_u32":
+                dv = A.n_dvvector_create(b"uint32_t", n, ctypes.c_void_p(vp_.data_ptr()))
+                try:
+                    check_i(A.n_sort_by_key(dk, dv, None))
+                    A.n_dvvector_to_host(dk, ctypes.c_void_p(ko.data_ptr()), 0, n)
+                    A.n_dvvector_to_host(dv, ctypes.c_void_p(vo.data_ptr()), 0, n)
+                finally:
+                    A.n_dv_destroy(dv)
+            elif wl == "inclusive_scan_i32":
+                check_i(A.n_inclusive_scan(dk, dk, None))
+                A.n_dvvector_to_host(dk, ctypes.c_void_p(ko.data_ptr()), 0, n)
+            else:
+                r = A.n_reduce(dk, None, None)
+                if not r:
+                    raise RuntimeError("n_reduce failed")
+                A.n_dv_destroy(r)
+        finally:
+            A.n_dv_destroy(dk)
+
+    for _ in range(2):
+        one()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    barrier()
+    secs = max_over_ranks(time.perf_counter() - t0)
+    if wl == "sort_by_key_u32":
+        kk = ko.numpy().view(np.uint32)
+        if n > 1 and not (kk[1:] >= kk[:-1]).all():
+            raise RuntimeError("e2e sort check failed")
+    return {"value": units_per_s_to_metric(wl, n * world * steps, secs), "unit": WORKLOADS[wl][5],
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": steps,
+            "ms_per_step": secs / steps * 1e3,
+            "path": "n_dvvector_create(pinned host) -> %s -> n_dvvector_to_host(pinned host)" %
+                    {"sort_by_key_u32": "n_sort_by_key", "inclusive_scan_i32": "n_inclusive_scan",
+                     "reduce_f32": "n_reduce"}[wl]}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sort_by_key_u32")
+    ap.add_argument("--n", type=int, default=0, help="override the element count (development only)")
+    ap.add_argument("--cpu-sample", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--allow-short-warmup", action="store_true")
+    args = ap.parse_args()
+    _, world, _ = dist_env()
+    if args.gpus != world and not (args.gpus == 1 and world == 1):
+        if world == 1:
+            raise SystemExit("bench.py: for --gpus N > 1 launch one process per GPU with torchrun")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -20,6 +20,13 @@ extern "C" {
 const char* trtc_last_error(void);
 /* number of thrustrtc_b200 kernels launched by this process */
 unsigned long long trtc_launch_count(void);
+/* optional per-launch timing: while enabled (on != 0; enabling or disabling discards old
+ * records) each launch of this library records a CUDA event on its stream.  count()
+ * synchronises those events and returns the number of timed launches (-1 on failure);
+ * get() returns the kernel name and its device time in milliseconds. */
+void trtc_timing_enable(int on);
+int trtc_timing_count(void);
+int trtc_timing_get(int i, char* name, unsigned long long name_cap, float* ms);
 /* synchronises `stream`; 0, or -1 when a kernel reported an error */
 int trtc_raw_sync(void* stream);
 

@@ -35,12 +35,12 @@ OPS = {"Plus": 0, "Maximum": 1, "Minimum": 2}
 
 
 def build(force=False):
-    """Compile trtc_oracle.cpp into oracle/liboracle.so (g++, -O2, OpenMP off)."""
+    """Compile trtc_oracle.cpp into oracle/liboracle.so (g++, -O2, std::thread)."""
     if (not force and os.path.exists(LIB)
             and os.path.getmtime(LIB) >= os.path.getmtime(SRC)):
         return LIB
     tmp = LIB + ".tmp"
-    subprocess.check_call(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", SRC, "-o", tmp])
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-pthread", SRC, "-o", tmp])
     os.replace(tmp, LIB)
     return LIB
 
@@ -66,6 +66,7 @@ def lib():
         L.oracle_reduce.argtypes = [i, i, vp, u64, vp, vp]
         L.oracle_reduce_f64.argtypes = [i, i, vp, u64, vp, vp]
         L.oracle_reduce_tree.argtypes = [i, i, vp, u64, vp, vp]
+        L.oracle_sort_pairs32.argtypes = [i, vp, vp, u64, i, i, vp, vp]
         _lib = L
     return _lib
 
@@ -110,6 +111,20 @@ def sort_perm(keys, descending=False, literal=False):
 
 def sort(keys, descending=False):
     return np.ascontiguousarray(keys)[sort_perm(keys, descending)]
+
+
+def sort_pairs32(keys, values, descending=False, threads=1):
+    """Sort_By_Key of 32-bit keys with 32-bit values on `threads` host threads (same order as
+    sort_by_key); the timed host baseline of the pair sort."""
+    keys = np.ascontiguousarray(keys)
+    values = np.ascontiguousarray(values)
+    assert keys.dtype.itemsize == 4 and values.dtype.itemsize == 4 and len(values) == len(keys)
+    ko, vo = np.empty_like(keys), np.empty_like(values)
+    r = lib().oracle_sort_pairs32(NP_CODES[keys.dtype], _ptr(keys), _ptr(values), len(keys),
+                                  1 if descending else 0, int(threads), _ptr(ko), _ptr(vo))
+    if r != 0:
+        raise ValueError("sort_pairs32: unsupported input")
+    return ko, vo
 
 
 def sort_by_key(keys, values, descending=False):

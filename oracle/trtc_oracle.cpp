@@ -14,6 +14,7 @@
 #include <vector>
 #include <algorithm>
 #include <numeric>
+#include <thread>
 
 namespace {
 
@@ -234,9 +235,80 @@ template <class T> T reduce_tree(int op, const T* in, uint64_t n, const T* init)
         default: return -1;                            \
     }
 
+// ---- the same stable order as sort_perm for 32-bit keys, computed with `threads` host
+// threads: (key' << 32 | index) packed in 64-bit words sorts stably with an unstable sort
+// (the index breaks ties); chunks are sorted in parallel and merged pairwise.  Used as the
+// timed host baseline of a pair sort; the order is that of internal/radix_sort.cpp:328-343.
+template <class T> void sort_pairs_packed(const T* keys, const uint32_t* vals, uint64_t n, int desc, int threads,
+                                          T* keys_out, uint32_t* vals_out) {
+    const uint64_t m = min_element_tree(keys, n);
+    const uint32_t dm = KeyW<T>::map(keys[m]);
+    std::vector<uint64_t> w(n), tmp(n);
+    if (threads < 1) threads = 1;
+    auto par = [&](auto&& fn) {
+        std::vector<std::thread> th;
+        for (int t = 0; t < threads; t++) th.emplace_back(fn, t);
+        for (auto& x : th) x.join();
+    };
+    par([&](int t) {
+        const uint64_t a = n * t / threads, b = n * (t + 1) / threads;
+        for (uint64_t i = a; i < b; i++) {
+            uint32_t k = (uint32_t)(KeyW<T>::map(keys[i]) - dm);
+            if (desc) k = ~k;  // descending by key', ties still by index
+            w[i] = ((uint64_t)k << 32) | i;
+        }
+        std::sort(w.begin() + a, w.begin() + b);
+    });
+    std::vector<uint64_t> bounds(threads + 1);
+    for (int t = 0; t <= threads; t++) bounds[t] = n * t / threads;
+    while (bounds.size() > 2) {
+        std::vector<uint64_t> nb;
+        std::vector<std::thread> th;
+        for (size_t j = 0; j + 1 < bounds.size(); j += 2) {
+            if (j + 2 < bounds.size()) {
+                const uint64_t a = bounds[j], mid = bounds[j + 1], b = bounds[j + 2];
+                th.emplace_back([&, a, mid, b] { std::merge(w.begin() + a, w.begin() + mid, w.begin() + mid, w.begin() + b, tmp.begin() + a); });
+                nb.push_back(a);
+            } else {
+                const uint64_t a = bounds[j], b = bounds[j + 1];
+                th.emplace_back([&, a, b] { std::copy(w.begin() + a, w.begin() + b, tmp.begin() + a); });
+                nb.push_back(a);
+            }
+        }
+        for (auto& x : th) x.join();
+        nb.push_back(n);
+        bounds.swap(nb);
+        w.swap(tmp);
+    }
+    par([&](int t) {
+        const uint64_t a = n * t / threads, b = n * (t + 1) / threads;
+        for (uint64_t i = a; i < b; i++) {
+            const uint64_t src = w[i] & 0xFFFFFFFFull;
+            keys_out[i] = keys[src];
+            vals_out[i] = vals[src];
+        }
+    });
+}
+
 }  // namespace
 
 extern "C" {
+
+// stable pair sort of 32-bit keys with 32-bit values on `threads` host threads (n < 2^32)
+int oracle_sort_pairs32(int type, const void* keys, const void* vals, unsigned long long n, int desc, int threads,
+                        void* keys_out, void* vals_out) {
+    if (n == 0) return 0;
+    if (n >= (1ull << 32)) return -1;
+    const uint32_t* v = (const uint32_t*)vals;
+    uint32_t* vo = (uint32_t*)vals_out;
+    switch (type) {
+        case T_I32: sort_pairs_packed<int32_t>((const int32_t*)keys, v, n, desc, threads, (int32_t*)keys_out, vo); break;
+        case T_U32: sort_pairs_packed<uint32_t>((const uint32_t*)keys, v, n, desc, threads, (uint32_t*)keys_out, vo); break;
+        case T_F32: sort_pairs_packed<float>((const float*)keys, v, n, desc, threads, (float*)keys_out, vo); break;
+        default: return -1;
+    }
+    return 0;
+}
 
 unsigned long long oracle_min_element(int type, const void* keys, unsigned long long n) {
     unsigned long long r = 0;

@@ -36,6 +36,9 @@ def _sig(name, restype, *argtypes):
 _sig("trtc_last_error", cstr)
 _sig("trtc_launch_count", u64)
 _sig("trtc_raw_sync", i32, vp)
+_sig("trtc_timing_enable", None, i32)
+_sig("trtc_timing_count", i32)
+_sig("trtc_timing_get", i32, i32, ctypes.c_char_p, u64, ctypes.POINTER(ctypes.c_float))
 _sig("trtc_raw_sort", i32, i32, vp, u64, i32, vp)
 _sig("trtc_raw_sort_by_key", i32, i32, vp, vp, u64, u64, i32, vp)
 _sig("trtc_raw_min_element", u64, i32, vp, u64, vp)
@@ -61,3 +64,22 @@ def last_error():
 def launch_count():
     """Number of thrustrtc_b200 kernels launched by this process so far."""
     return int(lib.trtc_launch_count())
+
+
+def timing_enable(on=True):
+    """Starts (or stops) recording the device time of every launch of this library."""
+    lib.trtc_timing_enable(1 if on else 0)
+
+
+def timing_records():
+    """[(kernel name, ms)] of the launches recorded since timing_enable(); synchronises."""
+    c = lib.trtc_timing_count()
+    if c < 0:
+        raise RuntimeError("timing: " + last_error())
+    out = []
+    buf = ctypes.create_string_buffer(256)
+    ms = ctypes.c_float()
+    for i in range(c):
+        if lib.trtc_timing_get(i, buf, 256, ctypes.byref(ms)) == 0:
+            out.append((buf.value.decode(), ms.value))
+    return out

@@ -334,45 +334,46 @@ __global__ void __launch_bounds__(BLOCK) scan_kernel(InV in, UOp uop, OutV out, 
         }
         if (lane == 0) { s_pre = tp; s_pre_has = tp_h ? 1 : 0; }
     }
-    if (MODE >= 2) return;
-    __syncthreads();
+    if constexpr (MODE < 2) {  // reductions write no elements
+        __syncthreads();
 
-    // warp prefix = tile prefix ⊕ aggregates of earlier warps
-    T wp = s_pre;
-    bool wp_h = s_pre_has != 0;
-    for (uint32_t w = 0; w < warp; w++) opt_combine(wp, wp_h, s_wagg[w], s_whas[w] != 0, op);
+        // warp prefix = tile prefix ⊕ aggregates of earlier warps
+        T wp = s_pre;
+        bool wp_h = s_pre_has != 0;
+        for (uint32_t w = 0; w < warp; w++) opt_combine(wp, wp_h, s_wagg[w], s_whas[w] != 0, op);
 
-    // ---- outputs
-    bool st_vec = false;
-    if constexpr (ViewTraits<OutV>::contiguous && VEC > 1 && sizeof(T) == sizeof(E))
-        st_vec = vec_ok && ((((size_t)out._data) & 15) == 0) && out._size >= n;
+        // ---- outputs
+        bool st_vec = false;
+        if constexpr (ViewTraits<OutV>::contiguous && VEC > 1 && sizeof(T) == sizeof(E))
+            st_vec = vec_ok && ((((size_t)out._data) & 15) == 0) && out._size >= n;
 #pragma unroll
-    for (int v = 0; v < NV; v++) {
-        T tp = wp;
-        bool tp_h = wp_h;
-        opt_combine(tp, tp_h, pre[v], pre_h[v], op);
-        T y[VEC];
+        for (int v = 0; v < NV; v++) {
+            T tp = wp;
+            bool tp_h = wp_h;
+            opt_combine(tp, tp_h, pre[v], pre_h[v], op);
+            T y[VEC];
 #pragma unroll
-        for (int e = 0; e < VEC; e++) {
-            if (MODE == 0) {
-                y[e] = tp_h ? (T)op(tp, x[v][e]) : x[v][e];
-            } else {
-                y[e] = (e == 0) ? tp : (T)op(tp, x[v][e - 1]);
+            for (int e = 0; e < VEC; e++) {
+                if (MODE == 0) {
+                    y[e] = tp_h ? (T)op(tp, x[v][e]) : x[v][e];
+                } else {
+                    y[e] = (e == 0) ? tp : (T)op(tp, x[v][e - 1]);
+                }
             }
-        }
-        if constexpr (ViewTraits<OutV>::contiguous && VEC > 1 && sizeof(T) == sizeof(E)) {
-            if (st_vec) {
-                union { uint4 q; T t[VEC]; } u;
+            if constexpr (ViewTraits<OutV>::contiguous && VEC > 1 && sizeof(T) == sizeof(E)) {
+                if (st_vec) {
+                    union { uint4 q; T t[VEC]; } u;
 #pragma unroll
-                for (int e = 0; e < VEC; e++) u.t[e] = y[e];
-                reinterpret_cast<uint4*>(out._data + tile_base + woff)[v * 32 + lane] = u.q;
-                continue;
+                    for (int e = 0; e < VEC; e++) u.t[e] = y[e];
+                    reinterpret_cast<uint4*>(out._data + tile_base + woff)[v * 32 + lane] = u.q;
+                    continue;
+                }
             }
-        }
 #pragma unroll
-        for (int e = 0; e < VEC; e++) {
-            const size_t r = woff + v * 32 * VEC + lane * VEC + e;
-            if (r < valid && tile_base + r < (size_t)out.size()) out[tile_base + r] = y[e];
+            for (int e = 0; e < VEC; e++) {
+                const size_t r = woff + v * 32 * VEC + lane * VEC + e;
+                if (r < valid && tile_base + r < (size_t)out.size()) out[tile_base + r] = y[e];
+            }
         }
     }
 }

@@ -1,6 +1,7 @@
 // api_raw.cpp -- raw-pointer C ABI (include/trtc_raw.h): built-in element types on device
 // buffers the caller owns, on a caller-chosen stream.  The object-model ABI of
 // include/thrustrtc_b200.h is layered on the same launchers.
+#include <cstring>
 #include "trtc_launch.h"
 #include "trtc_runtime.h"
 
@@ -13,6 +14,21 @@ extern "C" {
 const char* trtc_last_error() { return last_error(); }
 
 unsigned long long trtc_launch_count() { return launch_count(); }
+
+void trtc_timing_enable(int on) { ktimer_enable(on != 0); }
+int trtc_timing_count() { return ktimer_count(); }
+int trtc_timing_get(int i, char* name, unsigned long long name_cap, float* ms) {
+    std::string nm;
+    float t = 0.f;
+    if (!ktimer_get(i, nm, t)) return -1;
+    if (name && name_cap) {
+        const size_t c = nm.size() < name_cap - 1 ? nm.size() : (size_t)name_cap - 1;
+        memcpy(name, nm.data(), c);
+        name[c] = 0;
+    }
+    if (ms) *ms = t;
+    return 0;
+}
 
 // Copies the sort control block of `stream` (histograms, plan, NaN flag, rotation count of
 // the last sort on that stream) to host memory; for diagnostics.  Returns bytes copied.

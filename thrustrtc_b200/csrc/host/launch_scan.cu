@@ -37,9 +37,11 @@ static bool scan_t(const T* in, T* out, size_t n, const T* init, cudaStream_t s)
     VectorView<T> iv = make_view<T>(const_cast<T*>(in), n);
     VectorView<T> ov = make_view<T>(out, n);
     T ini = init ? *init : T();
+    ktimer_mark("", s);
     scan_kernel<VectorView<T>, Nothing, false, VectorView<T>, T, Op, MODE, SCAN_BLOCK, NV>
         <<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(iv, Nothing(), ov, n, Op(), ini, st);
     count_launch();
+    ktimer_mark("scan_kernel", s);
     return TRTC_CUDA(cudaGetLastError());
 }
 
@@ -87,10 +89,12 @@ static bool reduce_t(const T* in, size_t n, const T* init, void** result_dev, cu
     if (grid < 1) grid = 1;
     LookbackWs* w = reduce_ws(s, grid, sizeof(T));
     if (!w) return false;
+    ktimer_mark("", s);
     reduce_kernel<T, T, Op, Identity, false, BLOCK><<<(unsigned)grid, BLOCK, 0, s>>>(
         in, n, Op(), Identity(), (T*)w->partials, w->partial_has, w->done_ctr, (T*)w->result, init ? 1 : 0,
         init ? *init : T());
     count_launch();
+    ktimer_mark("reduce_kernel", s);
     *result_dev = w->result;
     return TRTC_CUDA(cudaGetLastError());
 }
@@ -142,9 +146,11 @@ static bool sbk_t(const K* keys, const T* vals, T* out, size_t n, const T* init,
     VectorView<T> vv = make_view<T>(const_cast<T*>(vals), n);
     VectorView<K> kv = make_view<K>(const_cast<K*>(keys), n);
     VectorView<T> ov = make_view<T>(out, n);
+    ktimer_mark("", s);
     scan_by_key_kernel<VectorView<K>, VectorView<T>, VectorView<T>, T, EqualTo, Plus, MODE, SCAN_BLOCK, NV>
         <<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(kv, vv, ov, n, EqualTo(), Plus(), init ? *init : T(), st);
     count_launch();
+    ktimer_mark("scan_by_key_kernel", s);
     return TRTC_CUDA(cudaGetLastError());
 }
 
@@ -186,10 +192,12 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
     if (!fill_lookback(st, s, tiles, 8)) return false;
     VectorView<T> iv = make_view<T>(const_cast<T*>(in), n);
     VectorView<T> ov = make_view<T>(out, n);
+    ktimer_mark("", s);
     compact_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing, Nothing, Nothing,
                    SCAN_BLOCK, ITEMS><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(
         iv, Nothing(), EqualTo(), value ? *value : T(), ov, Nothing(), Nothing(), Nothing(), n, st);
     count_launch();
+    ktimer_mark("compact_kernel", s);
     if (!TRTC_CUDA(cudaGetLastError())) return false;
     return TRTC_CUDA(cudaMemcpyAsync(count, st.result, 8, cudaMemcpyDeviceToHost, s)) &&
            check_device_errors(s, "compaction");

@@ -65,9 +65,12 @@ static bool radix_sort_run(K* keys, V* vals0, size_t n, cudaStream_t s, int vals
         size_t hgrid = (n + BLOCK * 16 - 1) / (BLOCK * 16);
         if (hgrid > (size_t)sms * 8) hgrid = (size_t)sms * 8;
         if (hgrid < 1) hgrid = 1;
+        ktimer_mark("", s);
         radix_hist_kernel<K, DESC, BLOCK><<<(unsigned)hgrid, BLOCK, 0, s>>>((const KB*)keys, n, ctrl, (uint4*)st0,
                                                                             status_bytes / 16);
+        ktimer_mark("radix_hist_kernel", s);
         radix_plan_kernel<D><<<1, 256, 0, s>>>(ctrl, n);
+        ktimer_mark("radix_plan_kernel", s);
         count_launch(2);
         if (FLOATKEY) {
             // the reference's Min_Element tree; only does work when a NaN was seen
@@ -94,18 +97,21 @@ static bool radix_sort_run(K* keys, V* vals0, size_t n, cudaStream_t s, int vals
             }
             radix_count_below_kernel<K, 256><<<(unsigned)(sms * 4), 256, 0, s>>>((const KB*)keys, n, ti[cur], ctrl);
             count_launch();
+            ktimer_mark("radix_nan_rotation", s);
         }
         const size_t smem = (size_t)TILE * sizeof(KB) + (HAS_VALS ? (size_t)TILE * sizeof(V) : 0) + (BLOCK / 32) * 256 * 4;
         auto pass_kernel = radix_pass_kernel<K, V, HAS_VALS, DESC, BLOCK, ITEMS, ST>;
         set_smem_attr_once(pass_kernel, smem);
         for (int p = 0; p < D; p++) {
             pass_kernel<<<(unsigned)tiles, BLOCK, smem, s>>>(bufs, n, ctrl, p, (ST*)st0, (ST*)st1, vals_from_index);
+            ktimer_mark("radix_pass_kernel", s);
         }
         count_launch(D);
         size_t cg = (n + 255) / 256;
         if (cg > (size_t)sms * 8) cg = (size_t)sms * 8;
         radix_copyback_kernel<K, V, HAS_VALS><<<(unsigned)cg, 256, 0, s>>>(bufs, n, ctrl);
         count_launch();
+        ktimer_mark("radix_copyback_kernel", s);
         ok = TRTC_CUDA(cudaGetLastError());
     }
     for (int i = 0; i < 2; i++) { tmp_free(tv[i], s); tmp_free(ti[i], s); }

@@ -164,7 +164,10 @@ bool jit_run(const std::vector<std::string>& headers, const std::string& kernel_
              const std::vector<ViewBuf>& params, unsigned smem = 0) {
     JitFunction f;
     if (!jit_get_kernel(headers, "", kernel_expr, "", f)) return false;
-    return jit_launch(f, dim_type{grid, 1, 1}, dim_type{block, 1, 1}, smem, S(), params);
+    ktimer_mark("", S());
+    const bool ok = jit_launch(f, dim_type{grid, 1, 1}, dim_type{block, 1, 1}, smem, S(), params);
+    ktimer_mark(("jit:" + kernel_expr.substr(0, kernel_expr.find('<'))).c_str(), S());
+    return ok;
 }
 
 // generic copy out[out_off + i] = in[in_off + i]

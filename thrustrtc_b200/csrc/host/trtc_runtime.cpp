@@ -6,6 +6,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <vector>
 
 namespace trtc_host {
 
@@ -26,6 +27,59 @@ bool cuda_ok(cudaError_t e, const char* what) {
 
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+struct KtMark { std::string name; cudaEvent_t ev; cudaStream_t s; };
+std::atomic<bool> g_kt_on{false};
+std::mutex g_kt_mu;
+std::vector<KtMark> g_kt;
+std::vector<cudaEvent_t> g_kt_free;
+std::vector<std::pair<std::string, float>> g_kt_done;
+}  // namespace
+
+void ktimer_enable(bool on) {
+    std::lock_guard<std::mutex> lk(g_kt_mu);
+    for (auto& m : g_kt) g_kt_free.push_back(m.ev);
+    g_kt.clear();
+    g_kt_done.clear();
+    g_kt_on.store(on, std::memory_order_relaxed);
+}
+
+void ktimer_mark(const char* name, cudaStream_t s) {
+    if (!g_kt_on.load(std::memory_order_relaxed)) return;
+    std::lock_guard<std::mutex> lk(g_kt_mu);
+    cudaEvent_t e;
+    if (!g_kt_free.empty()) { e = g_kt_free.back(); g_kt_free.pop_back(); }
+    else if (cudaEventCreate(&e) != cudaSuccess) return;
+    if (cudaEventRecord(e, s) != cudaSuccess) { g_kt_free.push_back(e); return; }
+    g_kt.push_back({name, e, s});
+}
+
+int ktimer_count() {
+    std::lock_guard<std::mutex> lk(g_kt_mu);
+    // resolve pending marks into (name, ms) pairs
+    for (size_t i = 0; i < g_kt.size(); i++) {
+        if (cudaEventSynchronize(g_kt[i].ev) != cudaSuccess) return -1;
+        if (g_kt[i].name.empty()) continue;
+        for (size_t j = i; j-- > 0;) {
+            if (g_kt[j].s != g_kt[i].s) continue;
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, g_kt[j].ev, g_kt[i].ev) == cudaSuccess) g_kt_done.push_back({g_kt[i].name, ms});
+            break;
+        }
+    }
+    for (auto& m : g_kt) g_kt_free.push_back(m.ev);
+    g_kt.clear();
+    return (int)g_kt_done.size();
+}
+
+bool ktimer_get(int i, std::string& name, float& ms) {
+    std::lock_guard<std::mutex> lk(g_kt_mu);
+    if (i < 0 || (size_t)i >= g_kt_done.size()) return false;
+    name = g_kt_done[i].first;
+    ms = g_kt_done[i].second;
+    return true;
+}
 
 int type_code_of(const std::string& c) {
     if (c == "int8_t" || c == "char" || c == "signed char") return TC_I8;

@@ -31,6 +31,15 @@ bool check_device_errors(cudaStream_t s, const char* what);  // syncs s, reads +
 void count_launch(unsigned n = 1);
 unsigned long long launch_count();
 
+// ---- optional per-launch timing (off by default).  While enabled, launchers record a CUDA
+// event on the launching stream after each kernel (ktimer_mark(name)); a mark with an empty
+// name only opens an interval.  The duration of a named mark is the time since the previous
+// mark on the same stream.
+void ktimer_enable(bool on);          // also discards recorded marks
+void ktimer_mark(const char* name, cudaStream_t s);
+int ktimer_count();                   // synchronises the recorded events
+bool ktimer_get(int i, std::string& name, float& ms);
+
 // ---- per-stream look-back workspace
 struct LookbackWs {
     uint32_t* flags = nullptr;
