@@ -41,6 +41,20 @@ unsigned long long trtc_raw_min_element(int type, const void* in, unsigned long 
 /* inclusive (exclusive=0) or exclusive scan with host-side init (NULL: zero) */
 int trtc_raw_scan(int type, int op, int exclusive, const void* in, void* out, unsigned long long n,
                   const void* init, void* stream);
+/* trtc_raw_scan without allocation.  No counterpart in the reference: ThrustRTC allocates
+ * its scan workspace on every call.  Same kernel and results as trtc_raw_scan for int32 (4),
+ * uint32 (5) and float (8), op 0 Plus / 1 Maximum / 2 Minimum, 1 <= n <= 2^28 elements; other
+ * sizes or types return -1 with a message in trtc_last_error() and launch nothing.  The
+ * look-back scratch is a 512 KiB array in the library's static device memory: the call
+ * allocates nothing (no cudaMalloc, cudaFree, pinned host memory or memory pool).  The first
+ * call on a device does a one-time set-up (the scratch array's address) and should precede
+ * stream capture.  status_dev: NULL, or a caller-owned device word that must be zero before
+ * the call; a device-side failure (an expired bounded wait) ORs a nonzero code into it.
+ * Calls share one scratch array per device, so calls that overlap on the device (other
+ * streams, other host threads) race: issue them in one stream or synchronise in between.
+ * Asynchronous with respect to the host. */
+int trtc_raw_scan_noalloc(int type, int op, int exclusive, const void* in, void* out, unsigned long long n,
+                          const void* init, unsigned int* status_dev, void* stream);
 /* reduction to host memory (init may be NULL); synchronous */
 int trtc_raw_reduce(int type, int op, const void* in, unsigned long long n, const void* init, void* result_host,
                     void* stream);
