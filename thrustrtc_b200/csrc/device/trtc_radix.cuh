@@ -87,67 +87,75 @@ __device__ inline uint32_t block_excl_scan_256(uint32_t v, uint32_t* s_wsum) {
 }
 
 // ------------------------------------------------------------------ histogram
+// One CTA per SM.  Every lane of a warp owns a private column of the shared histogram
+// (bin b of digit p at word (p*256 + b)*COPIES + lane % COPIES), so the shared-memory atomics
+// of a warp never collide on an address or a bank (COPIES = 32; 16 for 8-digit keys, whose
+// lanes l and l+16 may share a word), whatever the key distribution.  Loads are 16-byte
+// vectors, UNROLL of them in flight per thread.
+template <class K> struct HistCopies { enum { V = RadixKey<K>::DIGITS > 4 ? 16 : 32 }; };
+
 template <class K, bool DESC, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) radix_hist_kernel(const typename RadixKey<K>::B* __restrict__ keys, size_t n,
-                                                           SortCtrl* ctrl, uint4* status0, size_t status_vec4) {
+__global__ void __launch_bounds__(BLOCK, 1) radix_hist_kernel(const typename RadixKey<K>::B* __restrict__ keys, size_t n,
+                                                              SortCtrl* ctrl, uint4* status0, size_t status_vec4) {
     typedef RadixKey<K> RK;
     typedef typename RK::B KB;
     constexpr int D = RK::DIGITS;
-    __shared__ uint32_t sh[D][256];
+    constexpr int C = HistCopies<K>::V;
+    constexpr int VEC = 16 / (int)sizeof(KB);
+    constexpr int UNROLL = 4;
+    extern __shared__ __align__(16) uint32_t s_hist[];  // [D][256][C]
     __shared__ uint32_t s_nan;
-    for (int i = threadIdx.x; i < D * 256; i += BLOCK) (&sh[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < D * 256 * C; i += BLOCK) s_hist[i] = 0;
     if (threadIdx.x == 0) s_nan = 0;
-    __syncthreads();
 
     // clear the first look-back status array (the pass kernels clear the next one)
     for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < status_vec4; i += (size_t)gridDim.x * BLOCK)
         status0[i] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
 
-    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t* col = s_hist + (threadIdx.x & (C - 1));
     bool any_nan = false;
-    auto count_key = [&](KB k, bool valid) {
-        const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
-        if (!vmask) return;
-        const int src = __ffs(vmask) - 1;
-        if (valid) any_nan |= RK::is_nan(k);
+    auto count_key = [&](KB k) {
+        if (RK::is_nan(k)) any_nan = true;
         typename RK::U u = RK::ordered(k);
         if (DESC) u = ~u;
 #pragma unroll
         for (int p = 0; p < D; p++) {
-            const uint32_t d = (uint32_t)(u >> (8 * p)) & 0xFFu;
-            const uint32_t first = __shfl_sync(0xffffffffu, d, src);
-            if (__all_sync(0xffffffffu, !valid || d == first)) {
-                if ((int)lane == src) atomicAdd(&sh[p][first], (uint32_t)__popc(vmask));
-            } else if (valid) {
-                atomicAdd(&sh[p][d], 1u);
-            }
+            const uint32_t w = (p < 4) ? (uint32_t)u : (uint32_t)((unsigned long long)u >> 32);
+            const uint32_t d = __byte_perm(w, 0u, 0x4440u | (uint32_t)(p & 3));
+            atomicAdd(col + (p * 256 + d) * C, 1u);
         }
     };
 
-    constexpr int VEC = 16 / (int)sizeof(KB);
     const size_t nvec = ((((size_t)keys) & 15) == 0) ? n / VEC : 0;
-    const size_t warps_total = (size_t)gridDim.x * (BLOCK / 32);
-    const size_t gwarp = (size_t)blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5);
-    // vectorised body: each lane takes one 16-byte vector per round
-    for (size_t base = gwarp * 32; base < nvec; base += warps_total * 32) {
-        const size_t vi = base + lane;
-        const bool valid = vi < nvec;
-        union { uint4 q; KB k[VEC]; } u;
-        if (valid) u.q = reinterpret_cast<const uint4*>(keys)[vi];
+    const uint4* kv = reinterpret_cast<const uint4*>(keys);
+    const size_t stride = (size_t)gridDim.x * BLOCK;
+    size_t v = (size_t)blockIdx.x * BLOCK + threadIdx.x;
+    for (; v + (UNROLL - 1) * stride < nvec; v += UNROLL * stride) {
+        union { uint4 q; KB k[VEC]; } u[UNROLL];
 #pragma unroll
-        for (int e = 0; e < VEC; e++) count_key(valid ? u.k[e] : KB(0), valid);
+        for (int r = 0; r < UNROLL; r++) u[r].q = kv[v + r * stride];
+#pragma unroll
+        for (int r = 0; r < UNROLL; r++)
+#pragma unroll
+            for (int e = 0; e < VEC; e++) count_key(u[r].k[e]);
+    }
+    for (; v < nvec; v += stride) {
+        union { uint4 q; KB k[VEC]; } u;
+        u.q = kv[v];
+#pragma unroll
+        for (int e = 0; e < VEC; e++) count_key(u.k[e]);
     }
     // scalar tail (and unaligned inputs)
-    for (size_t base = nvec * VEC + gwarp * 32; base < n; base += warps_total * 32) {
-        const size_t i = base + lane;
-        const bool valid = i < n;
-        count_key(valid ? keys[i] : KB(0), valid);
-    }
+    for (size_t i = nvec * VEC + (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += stride) count_key(keys[i]);
     if (any_nan) s_nan = 1;
     __syncthreads();
-    for (int i = threadIdx.x; i < D * 256; i += BLOCK) {
-        const uint32_t c = (&sh[0][0])[i];
-        if (c) atomicAdd(&ctrl->hist[0][0] + i, c);
+    // fold the columns (rotated start: the lanes of a warp read different banks)
+    for (int b = threadIdx.x; b < D * 256; b += BLOCK) {
+        uint32_t sum = 0;
+#pragma unroll 8
+        for (int c = 0; c < C; c++) sum += s_hist[b * C + ((c + b) & (C - 1))];
+        if (sum) atomicAdd(&ctrl->hist[0][0] + b, sum);
     }
     if (threadIdx.x == 0 && s_nan) atomicOr(&ctrl->nan_flag, 1u);
 }
@@ -260,16 +268,50 @@ __global__ void __launch_bounds__(BLOCK) radix_count_below_kernel(const typename
 }
 
 // ------------------------------------------------------------------ one digit pass
+// Digit of byte `pass` of the ordered key code: one byte permute on the 32-bit half that
+// holds it (sel = 0x4440 | byte index within the half).
+template <class K, bool DESC>
+TRTC_FORCEINLINE uint32_t radix_digit_sel(typename RadixKey<K>::B k, uint32_t sel, bool hi) {
+    const typename RadixKey<K>::U u = RadixKey<K>::ordered(k);
+    uint32_t w;
+    if constexpr (sizeof(typename RadixKey<K>::U) == 8) w = hi ? (uint32_t)(u >> 32) : (uint32_t)u;
+    else w = (uint32_t)u;
+    const uint32_t d = __byte_perm(w, 0u, sel);
+    return DESC ? (d ^ 0xFFu) : d;
+}
+
+template <bool B> struct BoolC { static constexpr bool value = B; };
+
+#ifndef TRTC_RADIX_LB
+#define TRTC_RADIX_LB 16  // predecessor tiles polled per look-back round
+#endif
+
 // HAS_VALS: move a 4- or 8-byte payload with the keys.  vals_from_index: the payload of the
 // first active pass is the element index (used to sort a permutation for odd value sizes).
+//
+// Per tile (BLOCK threads x ITEMS keys, warp-striped: key i of lane l of warp w sits at
+// tile_base + w*32*ITEMS + i*32 + l):
+//   1. load the keys; rank every key inside its warp (peers of equal digit from 8 bit
+//      ballots, one shared-memory atomicAdd per peer group on the warp's digit counters);
+//   2. issue the payload loads (they complete while the counts are scanned);
+//   3. one thread per digit: tile count, publication of the tile aggregate, block-wide
+//      exclusive scan of the counts, warp offsets folded into the warp counters;
+//   4. stage keys (and payloads) in shared memory in digit order; then, one thread per
+//      digit, decoupled look-back for the digit's global offset, publication of the
+//      inclusive prefix, and a range check of the digit's destination run against n;
+//   5. write the tile out in bucket runs: consecutive threads write consecutive slots of a
+//      digit's run.
 template <class K, class V, bool HAS_VALS, bool DESC, int BLOCK, int ITEMS, class ST>
 __global__ void __launch_bounds__(BLOCK, (ITEMS >= 24 ? 2 : 3)) radix_pass_kernel(SortBufs bufs, size_t n, SortCtrl* ctrl, int pass,
                                                            ST* status0, ST* status1, int vals_from_index) {
-    static_assert(BLOCK >= 256, "one thread per digit is needed");
+    static_assert(BLOCK == 256, "one thread per digit");
     constexpr int TILE = BLOCK * ITEMS;
     constexpr int WARPS = BLOCK / 32;
+    constexpr bool FLOATKEY = is_same<K, float>::value || is_same<K, double>::value;
     typedef StatusBits<ST> SB;
     typedef typename RadixKey<K>::B KB;
+    // element positions: 32-bit while n < 2^30 (ST = uint32_t), else 64-bit
+    typedef typename conditional<(sizeof(ST) == 8), unsigned long long, uint32_t>::type IX;
     const SortPlan& plan = ctrl->plan;
     if (!((plan.active_mask >> pass) & 1u)) return;
 
@@ -277,7 +319,8 @@ __global__ void __launch_bounds__(BLOCK, (ITEMS >= 24 ? 2 : 3)) radix_pass_kerne
     KB* s_keys = reinterpret_cast<KB*>(smem);
     V* s_vals = reinterpret_cast<V*>(smem + sizeof(KB) * TILE);
     uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem + sizeof(KB) * TILE + (HAS_VALS ? sizeof(V) * TILE : 0));
-    __shared__ uint32_t s_count[256], s_start[256], s_adj[256], s_wsum[8];
+    __shared__ IX s_adj[256];
+    __shared__ uint32_t s_wsum[8];
     __shared__ uint32_t s_tile;
 
     const int ord = plan.ordinal[pass];
@@ -292,112 +335,115 @@ __global__ void __launch_bounds__(BLOCK, (ITEMS >= 24 ? 2 : 3)) radix_pass_kerne
     const V* __restrict__ src_v =
         reinterpret_cast<const V*>(ss == 0 ? bufs.vals[0] : (ss == 1 ? bufs.vals[1] : bufs.vals[2]));
     V* __restrict__ dst_v = reinterpret_cast<V*>(ds == 0 ? bufs.vals[0] : (ds == 1 ? bufs.vals[1] : bufs.vals[2]));
-    const int shift = pass * 8;
+    const uint32_t sel = 0x4440u | (uint32_t)(pass & 3);
+    const bool hi = pass >= 4;
     const bool index_payload = HAS_VALS && vals_from_index && ord == 0;
-    unsigned long long rot = 0;
-    if (pass == plan.last_pass && ctrl->rot_count) {
+    IX rot = 0;
+    if (FLOATKEY && pass == plan.last_pass && ctrl->rot_count) {
         const unsigned long long k = ctrl->rot_count % n;
-        rot = DESC ? k : (k ? n - k : 0);
+        rot = (IX)(DESC ? k : (k ? n - k : 0));
     }
 
     if (threadIdx.x == 0) s_tile = atomicAdd(&ctrl->tile_ctr[ord], 1u);
     for (int i = threadIdx.x; i < WARPS * 256; i += BLOCK) s_whist[i] = 0;
     __syncthreads();
     const size_t tile = s_tile;
-    for (int i = threadIdx.x; i < 256; i += BLOCK) st_next[tile * 256 + i] = 0;
+    st_next[tile * 256 + threadIdx.x] = 0;
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const size_t tile_base = tile * TILE;
     const size_t wbase = tile_base + (size_t)warp * 32 * ITEMS;
+    const KB* __restrict__ wk = src_k + wbase;
     const bool full = tile_base + TILE <= n;
+    const uint32_t tile_n = full ? (uint32_t)TILE : (uint32_t)(n - tile_base);
+    // keys of this warp inside the tile (partial tiles only)
+    const uint32_t warp_n = full ? 32u * ITEMS
+                                 : (tile_n > warp * 32u * ITEMS ? min(tile_n - warp * 32u * ITEMS, 32u * ITEMS) : 0u);
 
     KB keys[ITEMS];
     uint32_t rank[ITEMS];
-#pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-        const size_t idx = wbase + (size_t)i * 32 + lane;
-        keys[i] = (full || idx < n) ? src_k[idx] : KB(0);
-    }
-
-    // Warp multisplit ranking, stable within the warp (items in order, lanes in order).
-    // Per item: peers of the same digit (__match_any_sync), rank among them, and one
-    // shared-memory atomicAdd by the group leader that returns the warp's running count of
-    // that digit.  The atomics of successive items are independent instructions executed in
-    // issue order, so the items pipeline instead of forming a load->store chain.
-    uint32_t* wh = s_whist + warp * 256;
-    const uint32_t ltm = lanemask_lt();
-    uint32_t info[ITEMS];  // rank among peers | leader lane << 8
-#pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-        const size_t idx = wbase + (size_t)i * 32 + lane;
-        const uint32_t d = (full || idx < n) ? radix_digit<K, DESC>(keys[i], shift) : 256u;
-        // peers with the same digit: AND of 9 bit-ballots (cheaper than __match_any_sync on
-        // sm_100; the 9th bit separates the out-of-range slots of a partial tile)
-        uint32_t peers = 0xffffffffu;
-#pragma unroll
-        for (int b = 0; b < 9; b++) {
-            const uint32_t bit = (d >> b) & 1u;
-            const uint32_t bb = __ballot_sync(0xffffffffu, bit);
-            peers &= bit ? bb : ~bb;
-        }
-        const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
-        info[i] = (uint32_t)__popc(peers & ltm) | (leader << 8);
-        rank[i] = 0;
-        if (lane == leader && d < 256u) rank[i] = atomicAdd(&wh[d], (uint32_t)__popc(peers));
-    }
-#pragma unroll
-    for (int i = 0; i < ITEMS; i++)
-        rank[i] = __shfl_sync(0xffffffffu, rank[i], (int)(info[i] >> 8)) + (info[i] & 0xFFu);
-
-    // payloads are loaded only now (their registers were not needed during ranking)
     V vals[HAS_VALS ? ITEMS : 1];
-    if (HAS_VALS) {
+    uint32_t* wh = s_whist + warp * 256;
+
+    // ---- 1. load + warp multisplit ranking
+    auto rank_tile = [&](auto full_c) {
+        constexpr bool FULL = decltype(full_c)::value;
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
-            const size_t idx = wbase + (size_t)i * 32 + lane;
-            vals[i] = (full || idx < n) ? (index_payload ? (V)idx : src_v[idx]) : V();
+            const uint32_t r = (uint32_t)i * 32u + lane;
+            keys[i] = (FULL || r < warp_n) ? wk[r] : KB(0);
         }
-    }
+        const uint32_t ltm = lanemask_lt();
+        uint32_t info[ITEMS];  // rank among peers | group leader lane << 8
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t d = radix_digit_sel<K, DESC>(keys[i], sel, hi);
+            uint32_t peers = FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, (uint32_t)i * 32u + lane < warp_n);
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                const bool bit = (d >> b) & 1u;
+                const uint32_t bb = __ballot_sync(0xffffffffu, bit);
+                peers &= bit ? bb : ~bb;
+            }
+            // the highest lane of a group adds the group's size to the warp's digit counter
+            const uint32_t leader = 31u - __clz(peers);
+            info[i] = (uint32_t)__popc(peers & ltm) | (leader << 8);
+            rank[i] = 0;
+            if (lane == leader && (FULL || (uint32_t)i * 32u + lane < warp_n))
+                rank[i] = atomicAdd(&wh[d], (uint32_t)__popc(peers));
+        }
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++)
+            rank[i] = __shfl_sync(0xffffffffu, rank[i], (int)(info[i] >> 8)) + (info[i] & 0xFFu);
+        // ---- 2. payload loads, consumed only at staging
+        if constexpr (HAS_VALS) {
+            const V* __restrict__ wv = src_v + wbase;
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t r = (uint32_t)i * 32u + lane;
+                if (FULL || r < warp_n) vals[i] = index_payload ? (V)(wbase + r) : wv[r];
+            }
+        }
+    };
+    if (full) rank_tile(BoolC<true>());
+    else rank_tile(BoolC<false>());
     __syncthreads();
 
-    // per-digit tile counts, warp prefixes, publication of the tile aggregate
+    // ---- 3. one thread per digit: tile count, aggregate, block scan, warp offsets
+    const uint32_t d_me = threadIdx.x;
     uint32_t cnt = 0;
-    if (threadIdx.x < 256) {
-        const int d = threadIdx.x;
-        uint32_t sum = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; w++) cnt += s_whist[w * 256 + d_me];
+    st_relaxed(&st[tile * 256 + d_me], ((ST)(tile == 0 ? 2u : 1u) << SB::SHIFT) | (ST)cnt);
+    const uint32_t start = block_excl_scan_256<BLOCK>(cnt, s_wsum);
+    {
+        uint32_t run = start;
 #pragma unroll
         for (int w = 0; w < WARPS; w++) {
-            const uint32_t c = s_whist[w * 256 + d];
-            s_whist[w * 256 + d] = sum;
-            sum += c;
+            const uint32_t c = s_whist[w * 256 + d_me];
+            s_whist[w * 256 + d_me] = run;
+            run += c;
         }
-        cnt = sum;
-        s_count[d] = sum;
-        const ST flag = (ST)(tile == 0 ? 2u : 1u) << SB::SHIFT;
-        st_relaxed(&st[tile * 256 + d], flag | (ST)sum);
     }
-    const uint32_t start = block_excl_scan_256<BLOCK>(cnt, s_wsum);
-    if (threadIdx.x < 256) s_start[threadIdx.x] = start;
     __syncthreads();
 
-    // stage the tile in digit order
+    // ---- 4. stage in digit order
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
-        const size_t idx = wbase + (size_t)i * 32 + lane;
-        if (full || idx < n) {
-            const uint32_t d = radix_digit<K, DESC>(keys[i], shift);
-            const uint32_t pos = s_start[d] + wh[d] + rank[i];
+        if (full || (uint32_t)i * 32u + lane < warp_n) {
+            const uint32_t d = radix_digit_sel<K, DESC>(keys[i], sel, hi);
+            const uint32_t pos = wh[d] + rank[i];
             s_keys[pos] = keys[i];
             if (HAS_VALS) s_vals[pos] = vals[i];
         }
     }
 
-    // decoupled look-back, one thread per digit.  Each round trip polls LB predecessor tiles
-    // at once (independent loads), so the inclusive-prefix frontier advances LB tiles per
-    // memory round trip instead of one.
-    if (threadIdx.x < 256) {
-        constexpr int LB = 16;
-        const int d = threadIdx.x;
+    // ---- decoupled look-back for the digit's global offset.  Each round polls LB
+    // predecessor tiles at once (independent loads), so the inclusive-prefix frontier
+    // advances LB tiles per memory round trip.
+    bool bad = false;
+    {
+        constexpr int LB = TRTC_RADIX_LB;
         ST excl = 0;
         if (tile > 0) {
             long long j = (long long)tile - 1;  // newest tile not yet accumulated
@@ -407,7 +453,7 @@ __global__ void __launch_bounds__(BLOCK, (ITEMS >= 24 ? 2 : 3)) radix_pass_kerne
                 ST s[LB];
 #pragma unroll
                 for (int k = 0; k < LB; k++)
-                    s[k] = (j - k >= 0) ? ld_relaxed(&st[(size_t)(j - k) * 256 + d]) : ((ST)2u << SB::SHIFT);
+                    s[k] = (j - k >= 0) ? ld_relaxed(&st[(size_t)(j - k) * 256 + d_me]) : ((ST)2u << SB::SHIFT);
                 int used = 0;
 #pragma unroll
                 for (int k = 0; k < LB; k++) {
@@ -421,29 +467,42 @@ __global__ void __launch_bounds__(BLOCK, (ITEMS >= 24 ? 2 : 3)) radix_pass_kerne
                 j -= used;
                 if (!done && j < 0) done = true;
                 if (!done && used == 0) {
-                    if (!spin_continue(spins, bufs.err)) { report_error(bufs.err, TRTC_ERR_LOOKBACK_TIMEOUT); break; }
+                    if (!spin_continue(spins, bufs.err)) { report_error(bufs.err, TRTC_ERR_LOOKBACK_TIMEOUT); bad = true; break; }
                 }
             }
-            st_relaxed(&st[tile * 256 + d], ((ST)2u << SB::SHIFT) | (excl + (ST)s_count[d]));
+            st_relaxed(&st[tile * 256 + d_me], ((ST)2u << SB::SHIFT) | (excl + (ST)cnt));
         }
-        s_adj[d] = plan.base[pass][d] + (uint32_t)excl - s_start[d];
+        // the digit's destination run must lie inside [0, n)
+        const unsigned long long lo = (unsigned long long)plan.base[pass][d_me] + (unsigned long long)excl;
+        if (lo + cnt > (unsigned long long)n) bad = true;
+        s_adj[d_me] = (IX)lo - (IX)start;
     }
-    __syncthreads();
+    if (__syncthreads_or(bad)) {  // also completes the staging
+        if (threadIdx.x == 0) report_error(bufs.err, TRTC_ERR_BAD_PLAN);
+        return;
+    }
 
-    // write out in bucket runs
-    const uint32_t tile_n = full ? (uint32_t)TILE : (uint32_t)(n - tile_base);
-    for (uint32_t k = threadIdx.x; k < tile_n; k += BLOCK) {
-        const KB key = s_keys[k];
-        const uint32_t d = radix_digit<K, DESC>(key, shift);
-        unsigned long long dst = (uint32_t)(s_adj[d] + k);
-        if (rot) { dst += rot; if (dst >= n) dst -= n; }
-        if (dst < n) {
-            dst_k[dst] = key;
-            if (HAS_VALS) dst_v[dst] = s_vals[k];
-        } else {
-            report_error(bufs.err, TRTC_ERR_BAD_PLAN);
+    // ---- 5. write out in bucket runs
+    auto write_tile = [&](auto full_c) {
+        constexpr bool FULL = decltype(full_c)::value;
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t k = (uint32_t)i * BLOCK + threadIdx.x;
+            if (FULL || k < tile_n) {
+                const KB key = s_keys[k];
+                const uint32_t d = radix_digit_sel<K, DESC>(key, sel, hi);
+                IX dst = s_adj[d] + (IX)k;
+                if constexpr (FLOATKEY) {
+                    dst += rot;
+                    if (dst >= (IX)n) dst -= (IX)n;
+                }
+                dst_k[dst] = key;
+                if (HAS_VALS) dst_v[dst] = s_vals[k];
+            }
         }
-    }
+    };
+    if (full) write_tile(BoolC<true>());
+    else write_tile(BoolC<false>());
 }
 
 // single active pass: the result sits in temp A and is copied back to the caller's buffers

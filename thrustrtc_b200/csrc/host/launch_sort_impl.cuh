@@ -62,12 +62,15 @@ static bool radix_sort_run(K* keys, V* vals0, size_t n, cudaStream_t s, int vals
         bufs.err = device_error_word();
         cudaMemsetAsync(ctrl, 0, sizeof(SortCtrl), s);
         const int sms = sm_count();
-        size_t hgrid = (n + BLOCK * 16 - 1) / (BLOCK * 16);
-        if (hgrid > (size_t)sms * 8) hgrid = (size_t)sms * 8;
+        constexpr int HBLOCK = 1024;
+        size_t hgrid = (n + HBLOCK * 16 - 1) / (HBLOCK * 16);
+        if (hgrid > (size_t)sms) hgrid = (size_t)sms;
         if (hgrid < 1) hgrid = 1;
+        const size_t hsmem = (size_t)D * 256 * HistCopies<K>::V * 4;
+        auto hist_kernel = radix_hist_kernel<K, DESC, HBLOCK>;
+        set_smem_attr_once(hist_kernel, hsmem);
         ktimer_mark("", s);
-        radix_hist_kernel<K, DESC, BLOCK><<<(unsigned)hgrid, BLOCK, 0, s>>>((const KB*)keys, n, ctrl, (uint4*)st0,
-                                                                            status_bytes / 16);
+        hist_kernel<<<(unsigned)hgrid, HBLOCK, hsmem, s>>>((const KB*)keys, n, ctrl, (uint4*)st0, status_bytes / 16);
         ktimer_mark("radix_hist_kernel", s);
         radix_plan_kernel<D><<<1, 256, 0, s>>>(ctrl, n);
         ktimer_mark("radix_plan_kernel", s);
