@@ -13,7 +13,9 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [1, 2, 3, 255, 256, 257, 511, 512, 513, 4095, 4096, 4097, 65537, 1 << 20 | 7]
+# tile edges of the sort (256 x 20 keys for 4-byte keys, 256 x 8 for 8-byte keys) and the scans (4096)
+SIZES = [1, 2, 3, 255, 256, 257, 511, 512, 513, 2047, 2048, 2049, 4095, 4096, 4097, 5119, 5120, 5121, 10241,
+         65537, 1 << 20 | 7]
 NP_OF = {"int8_t": np.int8, "uint8_t": np.uint8, "int16_t": np.int16, "uint16_t": np.uint16,
          "int32_t": np.int32, "uint32_t": np.uint32, "int64_t": np.int64, "uint64_t": np.uint64,
          "float": np.float32, "double": np.float64}
@@ -73,7 +75,7 @@ def test_sort_keys(N, name, desc):
 @pytest.mark.parametrize("vsize", [4, 8, 1, 12])
 def test_sort_by_key(N, name, vsize):
     rng = np.random.default_rng(99)
-    for n in [1, 5, 4097, 100003, 1 << 20]:
+    for n in [1, 5, 4097, 5121, 100003, 1 << 20]:
         k = rand_keys(rng, name, n)
         if vsize in (4, 8):
             v = np.arange(n, dtype=np.uint32 if vsize == 4 else np.uint64)

@@ -282,8 +282,11 @@ TRTC_FORCEINLINE uint32_t radix_digit_sel(typename RadixKey<K>::B k, uint32_t se
 
 template <bool B> struct BoolC { static constexpr bool value = B; };
 
+#ifndef TRTC_RADIX_MINB  // resident CTAs per SM the pass kernel is compiled for
+#define TRTC_RADIX_MINB(items) ((items) >= 24 ? 2 : 3)
+#endif
 #ifndef TRTC_RADIX_LB
-#define TRTC_RADIX_LB 16  // predecessor tiles polled per look-back round
+#define TRTC_RADIX_LB 4  // predecessor tiles polled per look-back round
 #endif
 
 // HAS_VALS: move a 4- or 8-byte payload with the keys.  vals_from_index: the payload of the
@@ -302,7 +305,7 @@ template <bool B> struct BoolC { static constexpr bool value = B; };
 //   5. write the tile out in bucket runs: consecutive threads write consecutive slots of a
 //      digit's run.
 template <class K, class V, bool HAS_VALS, bool DESC, int BLOCK, int ITEMS, class ST>
-__global__ void __launch_bounds__(BLOCK, (ITEMS >= 24 ? 2 : 3)) radix_pass_kernel(SortBufs bufs, size_t n, SortCtrl* ctrl, int pass,
+__global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kernel(SortBufs bufs, size_t n, SortCtrl* ctrl, int pass,
                                                            ST* status0, ST* status1, int vals_from_index) {
     static_assert(BLOCK == 256, "one thread per digit");
     constexpr int TILE = BLOCK * ITEMS;

@@ -7,8 +7,12 @@
 
 namespace trtc_host {
 
-// items per thread of a digit pass (tile = 256 * ITEMS keys), from a sweep on B200 at 2^28 keys
-template <class K> struct SortTuning { enum { ITEMS = sizeof(K) >= 8 ? 8 : 16 }; };
+// items per thread of a digit pass (tile = 256 * ITEMS keys), from a sweep on B200 at 2^28
+// u32 pairs (16: 7.15 ms, 20: 7.01 ms, 24 with 2 CTAs/SM: 7.12 ms)
+#ifndef TRTC_RADIX_ITEMS32
+#define TRTC_RADIX_ITEMS32 20
+#endif
+template <class K> struct SortTuning { enum { ITEMS = sizeof(K) >= 8 ? 8 : TRTC_RADIX_ITEMS32 }; };
 
 // Opts a kernel in to `bytes` of dynamic shared memory (needed as soon as static +
 // dynamic exceeds 48 KB).  Tracked per kernel address: many instantiations share one type.
