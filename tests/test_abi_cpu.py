@@ -18,7 +18,7 @@ def _declared(header):
 
 @pytest.fixture(scope="module")
 def exported():
-    assert os.path.exists(LIB), "build the library first (python -m thrustrtc_b200.build)"
+    assert os.path.exists(LIB), "build the library first (python thrustrtc_b200/build.py)"
     out = subprocess.check_output(["nm", "-D", "--defined-only", LIB]).decode()
     return set(line.split()[-1] for line in out.splitlines() if line.strip())
 

@@ -11,7 +11,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libPyThrustRTC.so")
 
 if not os.path.exists(LIB_PATH):
-    raise ImportError("thrustrtc_b200: %s is missing; build it with `python -m thrustrtc_b200.build`" % LIB_PATH)
+    raise ImportError("thrustrtc_b200: %s is missing; build it with `python thrustrtc_b200/build.py`" % LIB_PATH)
 
 lib = ctypes.CDLL(LIB_PATH)
 

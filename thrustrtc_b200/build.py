@@ -7,7 +7,8 @@ library with the CUDA runtime linked statically (the driver is loaded at run tim
 library also loads on machines without a GPU).  The device headers are also embedded into
 the library as strings for the NVRTC path.
 
-Usage: python -m thrustrtc_b200.build [-j N] [--force]
+Usage: python thrustrtc_b200/build.py [-j N] [--force]
+(run as a script: importing the package needs the library this builds)
 """
 import argparse
 import concurrent.futures as cf

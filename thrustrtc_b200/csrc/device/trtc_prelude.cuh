@@ -117,6 +117,29 @@ TRTC_FORCEINLINE bool spin_continue(uint32_t& spins, const uint32_t* err) {
     return true;
 }
 
+// ------------------------------------------------------------------ L2 eviction hints
+// 16-byte global loads/stores with an L2 eviction-priority policy (createpolicy, sm_80+).
+TRTC_FORCEINLINE unsigned long long l2_evict_last_policy() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+TRTC_FORCEINLINE unsigned long long l2_evict_first_policy() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+TRTC_FORCEINLINE uint4 ld_l2hint(const uint4* a, unsigned long long pol) {
+    uint4 v;
+    asm volatile("ld.global.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(a), "l"(pol));
+    return v;
+}
+TRTC_FORCEINLINE void st_l2hint(uint4* a, const uint4& v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.v4.u32 [%0], {%1, %2, %3, %4}, %5;"
+                 :: "l"(a), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "l"(pol) : "memory");
+}
+
 // ------------------------------------------------------------------ radix key maps
 // RadixKey<K>::ordered(k) returns an unsigned code whose unsigned order is the order in
 // which the reference radix sort places keys (internal/radix_sort.cpp with the key maps of
@@ -194,6 +217,13 @@ template <class T> TRTC_FORCEINLINE T shfl_up_any(const T& v, int d) {
     a.t = v;
 #pragma unroll
     for (int i = 0; i < ShflWords<T>::N; i++) b.w[i] = __shfl_up_sync(0xffffffffu, a.w[i], d);
+    return b.t;
+}
+template <class T> TRTC_FORCEINLINE T shfl_xor_any(const T& v, int m) {
+    union U { T t; uint32_t w[ShflWords<T>::N]; TRTC_FORCEINLINE U() {} } a, b;
+    a.t = v;
+#pragma unroll
+    for (int i = 0; i < ShflWords<T>::N; i++) b.w[i] = __shfl_xor_sync(0xffffffffu, a.w[i], m);
     return b.t;
 }
 template <class T> TRTC_FORCEINLINE T shfl_down_any(const T& v, int d) {

@@ -57,7 +57,7 @@ TRTC_FORCEINLINE void opt_combine(T& a, bool& ah, const T& b, bool bh, Op& op) {
 // tiles start on 148 SMs.  Values of <= 4 bytes travel in the same 64-bit word as their
 // flag (no fence, no second load); larger values are read after one acquire fence.
 #ifndef TRTC_LB_K
-#define TRTC_LB_K 4
+#define TRTC_LB_K 1
 #endif
 template <class T> struct LbPack { static constexpr bool value = sizeof(T) <= 4; };
 
@@ -378,6 +378,233 @@ __global__ void __launch_bounds__(BLOCK) scan_kernel(InV in, UOp uop, OutV out, 
     }
 }
 
+// ---------------------------------------------------------------- two-phase tile scan
+// Contiguous inputs of built-in element types.  Each warp owns a contiguous segment of
+// 32 * ITEMS elements of the tile, read as ROWS rows of 32 lanes x one 16-byte vector.
+// Phase 1 reads the tile and reduces it (only the warp totals survive); warp 0 publishes the
+// tile aggregate and looks back.  Phase 2 reads the tile again -- it was read moments
+// earlier and is normally still in L2 -- and writes the scan.  No tile data is held in
+// registers across the look-back, so many tiles per SM wait at once and HBM keeps enough
+// loads in flight.  HBM traffic stays 4 B read + 4 B written per 4-byte element when the
+// re-read hits L2.  COMM: the operator is also commutative (the built-in Plus / Maximum /
+// Minimum), so phase 1 may fold each lane's vectors before the warp combines them.
+#ifndef TRTC_SCAN2_HINT
+#define TRTC_SCAN2_HINT 0
+#endif
+// Optional L2 policies: phase-1 lines are wanted again soon (evict last), phase-2 reads and
+// the output are not (evict first).  Measured slower on B200 than the plain loads and
+// streaming phase-2 loads / stores (0.614 vs 0.585 ms at 2^28 i32), so off by default.
+TRTC_FORCEINLINE uint4 ld_phase1(const uint4* p) {
+    if (TRTC_SCAN2_HINT) return ld_l2hint(p, l2_evict_last_policy());
+    return *p;
+}
+TRTC_FORCEINLINE uint4 ld_phase2(const uint4* p) {
+    if (TRTC_SCAN2_HINT) return ld_l2hint(p, l2_evict_first_policy());
+    return __ldcs(p);
+}
+TRTC_FORCEINLINE void st_out(uint4* p, const uint4& v) {
+    if (TRTC_SCAN2_HINT) st_l2hint(p, v, l2_evict_first_policy());
+    else __stcs(p, v);
+}
+
+template <class T, class Op, int MODE, int BLOCK, int ITEMS, bool COMM>
+__global__ void __launch_bounds__(BLOCK) scan2_kernel(const T* __restrict__ in, T* __restrict__ out, size_t n, Op op,
+                                                      T init, LookbackState st) {
+    constexpr int VEC = VecWidth<T>::V;
+    static_assert(VEC > 1 && ITEMS % VEC == 0, "16-byte vectors of T");
+    constexpr int ROWS = ITEMS / VEC;
+    constexpr int WARPS = BLOCK / 32;
+    constexpr int WSEG = 32 * ITEMS;
+    constexpr int TILE = BLOCK * ITEMS;
+    __shared__ uint32_t s_slot[2];
+    __shared__ T s_wtot[WARPS];
+    __shared__ int s_wh[WARPS];
+    __shared__ T s_woff[WARPS];
+    __shared__ int s_woh[WARPS];
+    __shared__ T s_pre;
+    __shared__ int s_pre_h;
+
+    const size_t tile = claim_tile(st, s_slot);
+    const size_t tile_base = tile * (size_t)TILE;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const long long wv = (long long)(n - tile_base) - (long long)warp * WSEG;
+    const uint32_t wvalid = wv <= 0 ? 0u : (wv >= WSEG ? (uint32_t)WSEG : (uint32_t)wv);
+    const bool aligned = ((((size_t)in) | ((size_t)out)) & 15) == 0;
+    const bool fast = aligned && wvalid == (uint32_t)WSEG;
+    const T* win = in + tile_base + (size_t)warp * WSEG;
+    T* wout = out + tile_base + (size_t)warp * WSEG;
+    typedef union { uint4 q; T t[VEC]; } Vec;
+
+    // ---- phase 1: warp totals (ordered: row by row, lanes in order within a row)
+    T wt = T();
+    bool wt_h = false;
+    if (fast) {
+        if constexpr (COMM) {
+            Vec v[ROWS];
+#pragma unroll
+            for (int r = 0; r < ROWS; r++) v[r].q = ld_phase1(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
+            T a = v[0].t[0];
+#pragma unroll
+            for (int r = 0; r < ROWS; r++)
+#pragma unroll
+                for (int e = 0; e < VEC; e++)
+                    if (r | e) a = (T)op(a, v[r].t[e]);
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) a = (T)op(a, shfl_xor_any(a, d));
+            wt = a;
+        } else {
+#pragma unroll
+            for (int r = 0; r < ROWS; r++) {
+                Vec v;
+                v.q = ld_phase1(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
+                T a = v.t[0];
+#pragma unroll
+                for (int e = 1; e < VEC; e++) a = (T)op(a, v.t[e]);
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {  // ordered tree: lane l combines l and l + d
+                    const T o = shfl_down_any(a, d);
+                    if ((lane & (2 * d - 1)) == 0) a = (T)op(a, o);
+                }
+                a = shfl_any(a, 0);
+                wt = r ? (T)op(wt, a) : a;
+            }
+        }
+        wt_h = true;
+    } else {
+        for (int r = 0; r < ROWS; r++) {
+            T a = T();
+            bool ah = false;
+#pragma unroll
+            for (int e = 0; e < VEC; e++) {
+                const uint32_t i = (uint32_t)r * 32u * VEC + lane * VEC + e;
+                if (i < wvalid) opt_combine(a, ah, win[i], true, op);
+            }
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const T o = shfl_down_any(a, d);
+                const bool oh = __shfl_down_sync(0xffffffffu, (int)ah, d) != 0 && lane + d < 32;
+                if ((lane & (2 * d - 1)) == 0) opt_combine(a, ah, o, oh, op);
+            }
+            a = shfl_any(a, 0);
+            ah = __shfl_sync(0xffffffffu, (int)ah, 0) != 0;
+            opt_combine(wt, wt_h, a, ah, op);
+        }
+    }
+    if (lane == 0) { s_wtot[warp] = wt; s_wh[warp] = wt_h ? 1 : 0; }
+    __syncthreads();
+
+    // ---- tile aggregate, look-back, tile prefix (warp 0)
+    if (warp == 0) {
+        T agg = T();
+        bool agg_h = false;
+        if (lane == 0) {
+            for (int w = 0; w < WARPS; w++) {
+                s_woff[w] = agg;
+                s_woh[w] = agg_h ? 1 : 0;
+                opt_combine(agg, agg_h, s_wtot[w], s_wh[w] != 0, op);
+            }
+        }
+        agg = shfl_any(agg, 0);
+        agg_h = __shfl_sync(0xffffffffu, (int)agg_h, 0) != 0;
+        T tp = T();
+        bool tp_h = false;
+        if (tile == 0) {
+            if (MODE == 1) { tp = init; tp_h = true; }
+            T incl = tp;
+            bool incl_h = tp_h;
+            opt_combine(incl, incl_h, agg, agg_h, op);
+            if (lane == 0) publish<T>(st, 0, incl, true, false);
+        } else {
+            if (lane == 0) publish<T>(st, tile, agg, false, false);
+            bool dummy;
+            const Opt<T> p = lookback_prefix<T, Op, false>(st, tile, op, dummy);
+            tp = p.v;
+            tp_h = p.h;
+            T incl = tp;
+            bool incl_h = tp_h;
+            opt_combine(incl, incl_h, agg, agg_h, op);
+            if (lane == 0) publish<T>(st, tile, incl, true, false);
+        }
+        if (lane == 0) { s_pre = tp; s_pre_h = tp_h ? 1 : 0; }
+    }
+    __syncthreads();
+
+    // ---- phase 2: re-read and write
+    T carry = s_pre;
+    bool carry_h = s_pre_h != 0;
+    opt_combine(carry, carry_h, s_woff[warp], s_woh[warp] != 0, op);
+    if (fast) {
+        Vec v2[ROWS];
+#pragma unroll
+        for (int r = 0; r < ROWS; r++) v2[r].q = ld_phase2(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
+#pragma unroll
+        for (int r = 0; r < ROWS; r++) {
+            T xi[VEC];  // inclusive within the lane's vector
+            xi[0] = v2[r].t[0];
+#pragma unroll
+            for (int e = 1; e < VEC; e++) xi[e] = (T)op(xi[e - 1], v2[r].t[e]);
+            T incl = xi[VEC - 1];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const T y = shfl_up_any(incl, d);
+                if (lane >= (uint32_t)d) incl = (T)op(y, incl);
+            }
+            const T ex = shfl_up_any(incl, 1);
+            const T row_tot = shfl_any(incl, 31);
+            // base = carry ⊕ (lanes before this one)
+            T base = ex;
+            bool base_h = lane > 0;
+            if (carry_h) { base = lane > 0 ? (T)op(carry, ex) : carry; base_h = true; }
+            Vec o;
+#pragma unroll
+            for (int e = 0; e < VEC; e++) {
+                if (MODE == 0) o.t[e] = base_h ? (T)op(base, xi[e]) : xi[e];
+                else o.t[e] = (e == 0) ? base : (T)op(base, xi[e - 1]);
+            }
+            st_out(reinterpret_cast<uint4*>(wout) + r * 32 + lane, o.q);
+            carry = carry_h ? (T)op(carry, row_tot) : row_tot;
+            carry_h = true;
+        }
+    } else {
+        for (int r = 0; r < ROWS; r++) {
+            const uint32_t i0 = (uint32_t)r * 32u * VEC + lane * VEC;
+            T xi[VEC];
+            T run = T();
+            bool run_h = false;
+#pragma unroll
+            for (int e = 0; e < VEC; e++) {
+                if (i0 + e < wvalid) opt_combine(run, run_h, win[i0 + e], true, op);
+                xi[e] = run;
+            }
+            T incl = run;
+            bool incl_h = run_h;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const T y = shfl_up_any(incl, d);
+                const bool yh = __shfl_up_sync(0xffffffffu, (int)incl_h, d) != 0;
+                if (lane >= (uint32_t)d && yh) { incl = incl_h ? (T)op(y, incl) : y; incl_h = true; }
+            }
+            const T ex = shfl_up_any(incl, 1);
+            const bool ex_h = __shfl_up_sync(0xffffffffu, (int)incl_h, 1) != 0 && lane > 0;
+            const T row_tot = shfl_any(incl, 31);
+            const bool row_h = __shfl_sync(0xffffffffu, (int)incl_h, 31) != 0;
+            T base = carry;
+            bool base_h = carry_h;
+            opt_combine(base, base_h, ex, ex_h, op);
+#pragma unroll
+            for (int e = 0; e < VEC; e++) {
+                if (i0 + e >= wvalid) continue;
+                T y;
+                if (MODE == 0) y = base_h ? (T)op(base, xi[e]) : xi[e];
+                else if (e == 0) y = base;
+                else y = base_h ? (T)op(base, xi[e - 1]) : xi[e - 1];
+                wout[i0 + e] = y;
+            }
+            opt_combine(carry, carry_h, row_tot, row_h, op);
+        }
+    }
+}
+
 // ---------------------------------------------------------------- segmented scan kernel
 // Segments continue at i while pred(key[i-1], key[i]) (default EqualTo; a head starts a new
 // segment).  MODE 0: inclusive.  MODE 1: exclusive, out[head] = init, otherwise
@@ -617,7 +844,18 @@ __global__ void __launch_bounds__(BLOCK) reduce_kernel(const E* __restrict__ in,
 #pragma unroll
         for (int e = 0; e < VEC; e++) acc[e] = get(u.e[e]);
         acc_h = true;
-        for (vi += gsz; vi < nvec; vi += gsz) {
+        // U independent 16-byte loads in flight per thread
+        constexpr int U = 4;
+        for (vi += gsz; vi + (U - 1) * gsz < nvec; vi += U * gsz) {
+            union { uint4 q; E e[VEC]; } w[U];
+#pragma unroll
+            for (int r = 0; r < U; r++) w[r].q = reinterpret_cast<const uint4*>(in)[vi + r * gsz];
+#pragma unroll
+            for (int r = 0; r < U; r++)
+#pragma unroll
+                for (int e = 0; e < VEC; e++) acc[e] = (T)op(acc[e], get(w[r].e[e]));
+        }
+        for (; vi < nvec; vi += gsz) {
             u.q = reinterpret_cast<const uint4*>(in)[vi];
 #pragma unroll
             for (int e = 0; e < VEC; e++) acc[e] = (T)op(acc[e], get(u.e[e]));
@@ -654,16 +892,30 @@ __global__ void __launch_bounds__(BLOCK) reduce_kernel(const E* __restrict__ in,
         s_last = prev == gridDim.x - 1;
     }
     __syncthreads();
-    if (s_last && threadIdx.x == 0) {
-        __threadfence();
-        T r = init;
-        bool rh = has_init != 0;
-        for (uint32_t b = 0; b < gridDim.x; b++) {
-            const T p = *(volatile T*)&partials[b];
-            const int ph = *(volatile int*)&partial_has[b];
-            opt_combine(r, rh, p, ph != 0, op);
-        }
-        *result = r;
+    if (!s_last) return;
+    // the last CTA folds the partials with all its threads (the operator is commutative)
+    __threadfence();
+    T r = T();
+    bool rh = false;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BLOCK) {
+        const T p = *(volatile T*)&partials[b];
+        const int ph = *(volatile int*)&partial_has[b];
+        opt_combine(r, rh, p, ph != 0, op);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        const T o = shfl_down_any(r, d);
+        const int oh = __shfl_down_sync(0xffffffffu, (int)rh, d);
+        if ((int)lane_id() + d < 32 && oh) { r = rh ? (T)op(r, o) : o; rh = true; }
+    }
+    __syncthreads();  // s_w / s_wh are reused
+    if (lane_id() == 0) { s_w[warp] = r; s_wh[warp] = rh ? 1 : 0; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T t = init;
+        bool th = has_init != 0;
+        for (int w = 0; w < WARPS; w++) opt_combine(t, th, s_w[w], s_wh[w] != 0, op);
+        *result = t;
         *done_ctr = 0;  // leaves the counter ready for the next call
     }
 }

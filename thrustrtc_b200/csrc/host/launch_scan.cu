@@ -27,22 +27,42 @@ static bool fill_lookback(LookbackState& st, cudaStream_t s, size_t tiles, size_
     return true;
 }
 
+#ifndef TRTC_SCAN2_ITEMS
+#define TRTC_SCAN2_ITEMS 32  // elements per thread of a two-phase scan tile (4-byte types)
+#endif
+
 template <class T, class Op, int MODE>
 static bool scan_t(const T* in, T* out, size_t n, const T* init, cudaStream_t s) {
-    constexpr int NV = scan_nv<T>();
-    constexpr int TILE = SCAN_BLOCK * NV * VecWidth<T>::V;
-    const size_t tiles = (n + TILE - 1) / TILE;
-    LookbackState st;
-    if (!fill_lookback(st, s, tiles, sizeof(T))) return false;
-    VectorView<T> iv = make_view<T>(const_cast<T*>(in), n);
-    VectorView<T> ov = make_view<T>(out, n);
     T ini = init ? *init : T();
-    ktimer_mark("", s);
-    scan_kernel<VectorView<T>, Nothing, false, VectorView<T>, T, Op, MODE, SCAN_BLOCK, NV>
-        <<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(iv, Nothing(), ov, n, Op(), ini, st);
-    count_launch();
-    ktimer_mark("scan_kernel", s);
-    return TRTC_CUDA(cudaGetLastError());
+    if constexpr (VecWidth<T>::V > 1) {
+        // two-phase tiles: TRTC_SCAN2_ITEMS elements per thread for 4-byte types, the same
+        // bytes per thread for other widths
+        constexpr int ITEMS = TRTC_SCAN2_ITEMS * 4 / (int)sizeof(T) < VecWidth<T>::V
+                                  ? VecWidth<T>::V : TRTC_SCAN2_ITEMS * 4 / (int)sizeof(T);
+        constexpr int TILE = SCAN_BLOCK * ITEMS;
+        const size_t tiles = (n + TILE - 1) / TILE;
+        LookbackState st;
+        if (!fill_lookback(st, s, tiles, sizeof(T))) return false;
+        ktimer_mark("", s);
+        scan2_kernel<T, Op, MODE, SCAN_BLOCK, ITEMS, true><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(in, out, n, Op(), ini, st);
+        count_launch();
+        ktimer_mark("scan_kernel", s);
+        return TRTC_CUDA(cudaGetLastError());
+    } else {
+        constexpr int NV = scan_nv<T>();
+        constexpr int TILE = SCAN_BLOCK * NV * VecWidth<T>::V;
+        const size_t tiles = (n + TILE - 1) / TILE;
+        LookbackState st;
+        if (!fill_lookback(st, s, tiles, sizeof(T))) return false;
+        VectorView<T> iv = make_view<T>(const_cast<T*>(in), n);
+        VectorView<T> ov = make_view<T>(out, n);
+        ktimer_mark("", s);
+        scan_kernel<VectorView<T>, Nothing, false, VectorView<T>, T, Op, MODE, SCAN_BLOCK, NV>
+            <<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(iv, Nothing(), ov, n, Op(), ini, st);
+        count_launch();
+        ktimer_mark("scan_kernel", s);
+        return TRTC_CUDA(cudaGetLastError());
+    }
 }
 
 template <class T>
