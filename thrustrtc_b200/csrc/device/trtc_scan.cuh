@@ -78,14 +78,15 @@ TRTC_FORCEINLINE uint32_t lb_state(uint32_t fw, uint32_t epoch8) {
     return (fw >= epoch8 && r < 8u && (r & 3u) != 0u && (r & 3u) != 3u) ? r : 0u;
 }
 
+// Ordered combination of tiles 0..j_start (walking back from j_start).
 template <class T, class Op, bool SEG>
-__device__ inline Opt<T> lookback_prefix(const LookbackState& st, size_t tile, Op& op, bool& seg_flag_out) {
+__device__ inline Opt<T> lookback_walk(const LookbackState& st, long long j_start, Op& op, bool& seg_flag_out) {
     constexpr int K = TRTC_LB_K;
     constexpr bool PACK = LbPack<T>::value;
     const uint32_t lane = lane_id();
     T acc = T();
     bool has = false, acc_head = false, done = false;
-    long long j0 = (long long)tile - 1;  // newest tile not yet combined
+    long long j0 = j_start;  // newest tile not yet combined
     while (!done && j0 >= 0) {
         // ---- poll K blocks of 32 tiles: lane l of block k holds tile j0 - 32k - l
         uint32_t code[K];
@@ -174,6 +175,11 @@ __device__ inline Opt<T> lookback_prefix(const LookbackState& st, size_t tile, O
     r.h = __shfl_sync(0xffffffffu, (int)has, 0) != 0;
     seg_flag_out = __shfl_sync(0xffffffffu, (int)acc_head, 0) != 0;
     return r;
+}
+
+template <class T, class Op, bool SEG>
+__device__ inline Opt<T> lookback_prefix(const LookbackState& st, size_t tile, Op& op, bool& seg_flag_out) {
+    return lookback_walk<T, Op, SEG>(st, (long long)tile - 1, op, seg_flag_out);
 }
 
 template <class T>
@@ -381,11 +387,12 @@ __global__ void __launch_bounds__(BLOCK) scan_kernel(InV in, UOp uop, OutV out, 
 // ---------------------------------------------------------------- two-phase tile scan
 // Contiguous inputs of built-in element types.  Each warp owns a contiguous segment of
 // 32 * ITEMS elements of the tile, read as ROWS rows of 32 lanes x one 16-byte vector.
-// Phase 1 reads the tile and reduces it (only the warp totals survive); warp 0 publishes the
-// tile aggregate and looks back.  Phase 2 reads the tile again -- it was read moments
-// earlier and is normally still in L2 -- and writes the scan.  No tile data is held in
-// registers across the look-back, so many tiles per SM wait at once and HBM keeps enough
-// loads in flight.  HBM traffic stays 4 B read + 4 B written per 4-byte element when the
+// Phase 1 reads the tile and reduces it (only the warp totals survive) and publishes the
+// tile aggregate.  Phase 2 looks back for the tile's prefix (warp 0), reads the tile again --
+// it was read moments earlier and is normally still in L2 -- and writes the scan.  CTAs are
+// persistent and software-pipelined: a CTA runs phase 1 of its next tile before the look-back
+// of its current one, so the look-back waits overlap HBM reads instead of idling the SM, and
+// no tile data is held in registers across a wait.  HBM traffic stays 4 B read + 4 B written per 4-byte element when the
 // re-read hits L2.  COMM: the operator is also commutative (the built-in Plus / Maximum /
 // Minimum), so phase 1 may fold each lane's vectors before the warp combines them.
 #ifndef TRTC_SCAN2_HINT
@@ -408,200 +415,239 @@ TRTC_FORCEINLINE void st_out(uint4* p, const uint4& v) {
 }
 
 template <class T, class Op, int MODE, int BLOCK, int ITEMS, bool COMM>
-__global__ void __launch_bounds__(BLOCK) scan2_kernel(const T* __restrict__ in, T* __restrict__ out, size_t n, Op op,
-                                                      T init, LookbackState st) {
+__global__ void __launch_bounds__(BLOCK) scan2_kernel(const T* __restrict__ in, T* __restrict__ out, size_t n,
+                                                      size_t tiles, Op op, T init, LookbackState st) {
     constexpr int VEC = VecWidth<T>::V;
     static_assert(VEC > 1 && ITEMS % VEC == 0, "16-byte vectors of T");
     constexpr int ROWS = ITEMS / VEC;
     constexpr int WARPS = BLOCK / 32;
     constexpr int WSEG = 32 * ITEMS;
     constexpr int TILE = BLOCK * ITEMS;
-    __shared__ uint32_t s_slot[2];
-    __shared__ T s_wtot[WARPS];
-    __shared__ int s_wh[WARPS];
-    __shared__ T s_woff[WARPS];
-    __shared__ int s_woh[WARPS];
+    typedef union { uint4 q; T t[VEC]; } Vec;
+    __shared__ unsigned long long s_ticket;
+    __shared__ T s_wtot[2][WARPS];
+    __shared__ int s_wh[2][WARPS];
+    __shared__ T s_woff[2][WARPS];
+    __shared__ int s_woh[2][WARPS];
+    __shared__ T s_agg[2];
+    __shared__ int s_agg_h[2];
     __shared__ T s_pre;
     __shared__ int s_pre_h;
 
-    const size_t tile = claim_tile(st, s_slot);
-    const size_t tile_base = tile * (size_t)TILE;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-    const long long wv = (long long)(n - tile_base) - (long long)warp * WSEG;
-    const uint32_t wvalid = wv <= 0 ? 0u : (wv >= WSEG ? (uint32_t)WSEG : (uint32_t)wv);
     const bool aligned = ((((size_t)in) | ((size_t)out)) & 15) == 0;
-    const bool fast = aligned && wvalid == (uint32_t)WSEG;
-    const T* win = in + tile_base + (size_t)warp * WSEG;
-    T* wout = out + tile_base + (size_t)warp * WSEG;
-    typedef union { uint4 q; T t[VEC]; } Vec;
 
-    // ---- phase 1: warp totals (ordered: row by row, lanes in order within a row)
-    T wt = T();
-    bool wt_h = false;
-    if (fast) {
-        if constexpr (COMM) {
-            Vec v[ROWS];
+    // Tickets are handed out in order; every CTA takes exactly one ticket >= tiles (which
+    // ends its loop), so the CTA that takes the last of the tiles + gridDim.x tickets resets
+    // the counter for the next launch on this stream.
+    auto claim = [&]() -> size_t {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned long long t = atomicAdd(st.tile_ctr, 1ull);
+            if (t == (unsigned long long)tiles + gridDim.x - 1) atomicExch(st.tile_ctr, 0ull);
+            s_ticket = t;
+        }
+        __syncthreads();
+        return (size_t)s_ticket;
+    };
+    auto warp_valid = [&](size_t tile) -> uint32_t {
+        const long long wv = (long long)(n - tile * (size_t)TILE) - (long long)warp * WSEG;
+        return wv <= 0 ? 0u : (wv >= WSEG ? (uint32_t)WSEG : (uint32_t)wv);
+    };
+
+    // ---- phase 1: warp totals (ordered), tile aggregate, publication
+    auto phase1 = [&](size_t tile, int b) {
+        const uint32_t wvalid = warp_valid(tile);
+        const bool fast = aligned && wvalid == (uint32_t)WSEG;
+        const T* win = in + tile * (size_t)TILE + (size_t)warp * WSEG;
+        T wt = T();
+        bool wt_h = false;
+        if (fast) {
+            if constexpr (COMM) {
+                Vec v[ROWS];
 #pragma unroll
-            for (int r = 0; r < ROWS; r++) v[r].q = ld_phase1(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
-            T a = v[0].t[0];
+                for (int r = 0; r < ROWS; r++) v[r].q = ld_phase1(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
+                T a = v[0].t[0];
 #pragma unroll
-            for (int r = 0; r < ROWS; r++)
+                for (int r = 0; r < ROWS; r++)
 #pragma unroll
-                for (int e = 0; e < VEC; e++)
-                    if (r | e) a = (T)op(a, v[r].t[e]);
+                    for (int e = 0; e < VEC; e++)
+                        if (r | e) a = (T)op(a, v[r].t[e]);
 #pragma unroll
-            for (int d = 16; d > 0; d >>= 1) a = (T)op(a, shfl_xor_any(a, d));
-            wt = a;
+                for (int d = 16; d > 0; d >>= 1) a = (T)op(a, shfl_xor_any(a, d));
+                wt = a;
+            } else {
+#pragma unroll
+                for (int r = 0; r < ROWS; r++) {
+                    Vec v;
+                    v.q = ld_phase1(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
+                    T a = v.t[0];
+#pragma unroll
+                    for (int e = 1; e < VEC; e++) a = (T)op(a, v.t[e]);
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {  // ordered tree: lane l combines l and l + d
+                        const T o = shfl_down_any(a, d);
+                        if ((lane & (2 * d - 1)) == 0) a = (T)op(a, o);
+                    }
+                    a = shfl_any(a, 0);
+                    wt = r ? (T)op(wt, a) : a;
+                }
+            }
+            wt_h = true;
         } else {
-#pragma unroll
             for (int r = 0; r < ROWS; r++) {
-                Vec v;
-                v.q = ld_phase1(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
-                T a = v.t[0];
+                T a = T();
+                bool ah = false;
 #pragma unroll
-                for (int e = 1; e < VEC; e++) a = (T)op(a, v.t[e]);
+                for (int e = 0; e < VEC; e++) {
+                    const uint32_t i = (uint32_t)r * 32u * VEC + lane * VEC + e;
+                    if (i < wvalid) opt_combine(a, ah, win[i], true, op);
+                }
 #pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {  // ordered tree: lane l combines l and l + d
+                for (int d = 1; d < 32; d <<= 1) {
                     const T o = shfl_down_any(a, d);
-                    if ((lane & (2 * d - 1)) == 0) a = (T)op(a, o);
+                    const bool oh = __shfl_down_sync(0xffffffffu, (int)ah, d) != 0 && lane + d < 32;
+                    if ((lane & (2 * d - 1)) == 0) opt_combine(a, ah, o, oh, op);
                 }
                 a = shfl_any(a, 0);
-                wt = r ? (T)op(wt, a) : a;
+                ah = __shfl_sync(0xffffffffu, (int)ah, 0) != 0;
+                opt_combine(wt, wt_h, a, ah, op);
             }
         }
-        wt_h = true;
-    } else {
-        for (int r = 0; r < ROWS; r++) {
-            T a = T();
-            bool ah = false;
-#pragma unroll
-            for (int e = 0; e < VEC; e++) {
-                const uint32_t i = (uint32_t)r * 32u * VEC + lane * VEC + e;
-                if (i < wvalid) opt_combine(a, ah, win[i], true, op);
-            }
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const T o = shfl_down_any(a, d);
-                const bool oh = __shfl_down_sync(0xffffffffu, (int)ah, d) != 0 && lane + d < 32;
-                if ((lane & (2 * d - 1)) == 0) opt_combine(a, ah, o, oh, op);
-            }
-            a = shfl_any(a, 0);
-            ah = __shfl_sync(0xffffffffu, (int)ah, 0) != 0;
-            opt_combine(wt, wt_h, a, ah, op);
-        }
-    }
-    if (lane == 0) { s_wtot[warp] = wt; s_wh[warp] = wt_h ? 1 : 0; }
-    __syncthreads();
-
-    // ---- tile aggregate, look-back, tile prefix (warp 0)
-    if (warp == 0) {
-        T agg = T();
-        bool agg_h = false;
-        if (lane == 0) {
+        if (lane == 0) { s_wtot[b][warp] = wt; s_wh[b][warp] = wt_h ? 1 : 0; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            T agg = T();
+            bool agg_h = false;
             for (int w = 0; w < WARPS; w++) {
-                s_woff[w] = agg;
-                s_woh[w] = agg_h ? 1 : 0;
-                opt_combine(agg, agg_h, s_wtot[w], s_wh[w] != 0, op);
+                s_woff[b][w] = agg;
+                s_woh[b][w] = agg_h ? 1 : 0;
+                opt_combine(agg, agg_h, s_wtot[b][w], s_wh[b][w] != 0, op);
+            }
+            s_agg[b] = agg;
+            s_agg_h[b] = agg_h ? 1 : 0;
+            if (tile == 0) {
+                T incl = init;
+                bool incl_h = MODE == 1;
+                if (!incl_h) incl = T();
+                opt_combine(incl, incl_h, agg, agg_h, op);
+                publish<T>(st, 0, incl, true, false);
+            } else {
+                publish<T>(st, tile, agg, false, false);
             }
         }
-        agg = shfl_any(agg, 0);
-        agg_h = __shfl_sync(0xffffffffu, (int)agg_h, 0) != 0;
-        T tp = T();
-        bool tp_h = false;
-        if (tile == 0) {
-            if (MODE == 1) { tp = init; tp_h = true; }
-            T incl = tp;
-            bool incl_h = tp_h;
-            opt_combine(incl, incl_h, agg, agg_h, op);
-            if (lane == 0) publish<T>(st, 0, incl, true, false);
-        } else {
-            if (lane == 0) publish<T>(st, tile, agg, false, false);
-            bool dummy;
-            const Opt<T> p = lookback_prefix<T, Op, false>(st, tile, op, dummy);
-            tp = p.v;
-            tp_h = p.h;
-            T incl = tp;
-            bool incl_h = tp_h;
-            opt_combine(incl, incl_h, agg, agg_h, op);
-            if (lane == 0) publish<T>(st, tile, incl, true, false);
-        }
-        if (lane == 0) { s_pre = tp; s_pre_h = tp_h ? 1 : 0; }
-    }
-    __syncthreads();
+    };
 
-    // ---- phase 2: re-read and write
-    T carry = s_pre;
-    bool carry_h = s_pre_h != 0;
-    opt_combine(carry, carry_h, s_woff[warp], s_woh[warp] != 0, op);
-    if (fast) {
-        Vec v2[ROWS];
-#pragma unroll
-        for (int r = 0; r < ROWS; r++) v2[r].q = ld_phase2(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
-#pragma unroll
-        for (int r = 0; r < ROWS; r++) {
-            T xi[VEC];  // inclusive within the lane's vector
-            xi[0] = v2[r].t[0];
-#pragma unroll
-            for (int e = 1; e < VEC; e++) xi[e] = (T)op(xi[e - 1], v2[r].t[e]);
-            T incl = xi[VEC - 1];
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const T y = shfl_up_any(incl, d);
-                if (lane >= (uint32_t)d) incl = (T)op(y, incl);
+
+    size_t cur = claim();
+    if (cur >= tiles) return;
+    int buf = 0;
+    phase1(cur, 0);
+    while (true) {
+        const size_t nxt = claim();
+        if (nxt < tiles) phase1(nxt, buf ^ 1);
+        // look-back of the current tile (warp 0)
+        if (warp == 0) {
+            T tp = T();
+            bool tp_h = false;
+            if (cur == 0) {
+                if (MODE == 1) { tp = init; tp_h = true; }
+            } else {
+                bool dummy;
+                const Opt<T> p = lookback_prefix<T, Op, false>(st, cur, op, dummy);
+                tp = p.v;
+                tp_h = p.h;
+                T incl = tp;
+                bool incl_h = tp_h;
+                opt_combine(incl, incl_h, s_agg[buf], s_agg_h[buf] != 0, op);
+                if (lane == 0) publish<T>(st, cur, incl, true, false);
             }
-            const T ex = shfl_up_any(incl, 1);
-            const T row_tot = shfl_any(incl, 31);
-            // base = carry ⊕ (lanes before this one)
-            T base = ex;
-            bool base_h = lane > 0;
-            if (carry_h) { base = lane > 0 ? (T)op(carry, ex) : carry; base_h = true; }
-            Vec o;
-#pragma unroll
-            for (int e = 0; e < VEC; e++) {
-                if (MODE == 0) o.t[e] = base_h ? (T)op(base, xi[e]) : xi[e];
-                else o.t[e] = (e == 0) ? base : (T)op(base, xi[e - 1]);
-            }
-            st_out(reinterpret_cast<uint4*>(wout) + r * 32 + lane, o.q);
-            carry = carry_h ? (T)op(carry, row_tot) : row_tot;
-            carry_h = true;
+            if (lane == 0) { s_pre = tp; s_pre_h = tp_h ? 1 : 0; }
         }
-    } else {
-        for (int r = 0; r < ROWS; r++) {
-            const uint32_t i0 = (uint32_t)r * 32u * VEC + lane * VEC;
-            T xi[VEC];
-            T run = T();
-            bool run_h = false;
+        __syncthreads();
+        // re-read and write the current tile
+        {
+            const uint32_t wvalid = warp_valid(cur);
+            const bool fast = aligned && wvalid == (uint32_t)WSEG;
+            const T* win = in + cur * (size_t)TILE + (size_t)warp * WSEG;
+            T* wout = out + cur * (size_t)TILE + (size_t)warp * WSEG;
+            T carry = s_pre;
+            bool carry_h = s_pre_h != 0;
+            opt_combine(carry, carry_h, s_woff[buf][warp], s_woh[buf][warp] != 0, op);
+            if (fast) {
+                Vec v2[ROWS];
 #pragma unroll
-            for (int e = 0; e < VEC; e++) {
-                if (i0 + e < wvalid) opt_combine(run, run_h, win[i0 + e], true, op);
-                xi[e] = run;
-            }
-            T incl = run;
-            bool incl_h = run_h;
+                for (int r = 0; r < ROWS; r++) v2[r].q = ld_phase2(reinterpret_cast<const uint4*>(win) + r * 32 + lane);
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const T y = shfl_up_any(incl, d);
-                const bool yh = __shfl_up_sync(0xffffffffu, (int)incl_h, d) != 0;
-                if (lane >= (uint32_t)d && yh) { incl = incl_h ? (T)op(y, incl) : y; incl_h = true; }
-            }
-            const T ex = shfl_up_any(incl, 1);
-            const bool ex_h = __shfl_up_sync(0xffffffffu, (int)incl_h, 1) != 0 && lane > 0;
-            const T row_tot = shfl_any(incl, 31);
-            const bool row_h = __shfl_sync(0xffffffffu, (int)incl_h, 31) != 0;
-            T base = carry;
-            bool base_h = carry_h;
-            opt_combine(base, base_h, ex, ex_h, op);
+                for (int r = 0; r < ROWS; r++) {
+                    T xi[VEC];  // inclusive within the lane's vector
+                    xi[0] = v2[r].t[0];
 #pragma unroll
-            for (int e = 0; e < VEC; e++) {
-                if (i0 + e >= wvalid) continue;
-                T y;
-                if (MODE == 0) y = base_h ? (T)op(base, xi[e]) : xi[e];
-                else if (e == 0) y = base;
-                else y = base_h ? (T)op(base, xi[e - 1]) : xi[e - 1];
-                wout[i0 + e] = y;
+                    for (int e = 1; e < VEC; e++) xi[e] = (T)op(xi[e - 1], v2[r].t[e]);
+                    T incl = xi[VEC - 1];
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const T y = shfl_up_any(incl, d);
+                        if (lane >= (uint32_t)d) incl = (T)op(y, incl);
+                    }
+                    const T ex = shfl_up_any(incl, 1);
+                    const T row_tot = shfl_any(incl, 31);
+                    // base = carry ⊕ (lanes before this one)
+                    T base = ex;
+                    bool base_h = lane > 0;
+                    if (carry_h) { base = lane > 0 ? (T)op(carry, ex) : carry; base_h = true; }
+                    Vec o;
+#pragma unroll
+                    for (int e = 0; e < VEC; e++) {
+                        if (MODE == 0) o.t[e] = base_h ? (T)op(base, xi[e]) : xi[e];
+                        else o.t[e] = (e == 0) ? base : (T)op(base, xi[e - 1]);
+                    }
+                    st_out(reinterpret_cast<uint4*>(wout) + r * 32 + lane, o.q);
+                    carry = carry_h ? (T)op(carry, row_tot) : row_tot;
+                    carry_h = true;
+                }
+            } else {
+                for (int r = 0; r < ROWS; r++) {
+                    const uint32_t i0 = (uint32_t)r * 32u * VEC + lane * VEC;
+                    T xi[VEC];
+                    T run = T();
+                    bool run_h = false;
+#pragma unroll
+                    for (int e = 0; e < VEC; e++) {
+                        if (i0 + e < wvalid) opt_combine(run, run_h, win[i0 + e], true, op);
+                        xi[e] = run;
+                    }
+                    T incl = run;
+                    bool incl_h = run_h;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const T y = shfl_up_any(incl, d);
+                        const bool yh = __shfl_up_sync(0xffffffffu, (int)incl_h, d) != 0;
+                        if (lane >= (uint32_t)d && yh) { incl = incl_h ? (T)op(y, incl) : y; incl_h = true; }
+                    }
+                    const T ex = shfl_up_any(incl, 1);
+                    const bool ex_h = __shfl_up_sync(0xffffffffu, (int)incl_h, 1) != 0 && lane > 0;
+                    const T row_tot = shfl_any(incl, 31);
+                    const bool row_h = __shfl_sync(0xffffffffu, (int)incl_h, 31) != 0;
+                    T base = carry;
+                    bool base_h = carry_h;
+                    opt_combine(base, base_h, ex, ex_h, op);
+#pragma unroll
+                    for (int e = 0; e < VEC; e++) {
+                        if (i0 + e >= wvalid) continue;
+                        T y;
+                        if (MODE == 0) y = base_h ? (T)op(base, xi[e]) : xi[e];
+                        else if (e == 0) y = base;
+                        else y = base_h ? (T)op(base, xi[e - 1]) : xi[e - 1];
+                        wout[i0 + e] = y;
+                    }
+                    opt_combine(carry, carry_h, row_tot, row_h, op);
+                }
             }
-            opt_combine(carry, carry_h, row_tot, row_h, op);
         }
+        if (nxt >= tiles) break;
+        cur = nxt;
+        buf ^= 1;
     }
 }
 

@@ -43,8 +43,15 @@ static bool scan_t(const T* in, T* out, size_t n, const T* init, cudaStream_t s)
         const size_t tiles = (n + TILE - 1) / TILE;
         LookbackState st;
         if (!fill_lookback(st, s, tiles, sizeof(T))) return false;
+        // persistent CTAs: as many as fit on the device at once
+        auto kernel = scan2_kernel<T, Op, MODE, SCAN_BLOCK, ITEMS, true>;
+        static int per_sm = 0;
+        if (per_sm == 0 && !TRTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, SCAN_BLOCK, 0)))
+            return false;
+        size_t grid = (size_t)(per_sm > 0 ? per_sm : 1) * sm_count();
+        if (grid > tiles) grid = tiles;
         ktimer_mark("", s);
-        scan2_kernel<T, Op, MODE, SCAN_BLOCK, ITEMS, true><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(in, out, n, Op(), ini, st);
+        kernel<<<(unsigned)grid, SCAN_BLOCK, 0, s>>>(in, out, n, tiles, Op(), ini, st);
         count_launch();
         ktimer_mark("scan_kernel", s);
         return TRTC_CUDA(cudaGetLastError());
