@@ -39,12 +39,13 @@ HBM_FALLBACK_GBS = 6650.0
 L2_BYTES = 126 * 1024 * 1024
 
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant kernel,
-# per unit processed (bytes per pair / element); None until a capture of the current kernel
-# exists.  Source summaries: profiles/<kernel>_<workload>.md
+# per unit processed (bytes per pair / element), from captures of smaller cases above L2
+# scaled by the units processed (traffic grows in proportion).  Source summaries:
+# profiles/<kernel>_<workload>.md
 NCU_TRAFFIC_PER_UNIT = {
-    "sort_by_key_u32": None,
-    "inclusive_scan_i32": None,
-    "reduce_f32": None,
+    "sort_by_key_u32": 15.75,   # radix_pass_kernel, 2^25 pairs: (269.8 + 258.6) MB / 2^25
+    "inclusive_scan_i32": 7.15,  # scan2_kernel, 2^26 elements: (270.8 + 208.7) MB / 2^26
+    "reduce_f32": 4.07,          # reduce_kernel, 2^26 elements: (268.5 + 4.9) MB / 2^26
 }
 
 WORKLOADS = {
