@@ -69,6 +69,27 @@ unsigned long long trtc_raw_remove_copy(int type, const void* in, void* out, uns
                                         const void* value, void* stream);
 unsigned long long trtc_raw_unique_copy(int type, const void* in, void* out, unsigned long long n, void* stream);
 
+/* Batched segmented sort + scan (no reference counterpart; the reference needs one sort call
+ * and one scan call per segment).  Segment i is keys/values[offsets[i], offsets[i+1]) with
+ * `offsets` a device array of nseg + 1 ascending element indices.  Each segment is stably
+ * sorted by key (ascending or descending, same order as trtc_raw_sort_by_key on it alone),
+ * its 4-byte values move with the keys, and scan_out receives the exclusive Plus scan
+ * (uint32 wrap-around) of each segment's sorted values.  Key types 4 (int32), 5 (uint32),
+ * 8 (float), 6 (int64), 7 (uint64); n and nseg below 2^32.  One persistent launch over all
+ * segments; the caller passes a device workspace of at least
+ * trtc_raw_segmented_workspace_bytes(key_type, n, nseg) bytes, and the call allocates nothing
+ * else (it can be captured in a CUDA graph after a first, uncaptured call of the same key
+ * type has set the kernels up). */
+unsigned long long trtc_raw_segmented_workspace_bytes(int key_type, unsigned long long n, unsigned long long nseg);
+int trtc_raw_segmented_sort_scan(int key_type, void* keys, void* values, void* scan_out,
+                                 const unsigned long long* offsets, unsigned long long nseg, unsigned long long n,
+                                 void* workspace, unsigned long long workspace_bytes, int descending, void* stream);
+/* Times the tile configurations (256 x 8 or 256 x 16 keys for the on-chip class) on random
+ * keys with these segment offsets and keeps the faster one for this key type; returns the
+ * chosen items per thread, or -1.  Allocates its own scratch; synchronous. */
+int trtc_raw_segmented_autotune(int key_type, const unsigned long long* offsets, unsigned long long nseg,
+                                unsigned long long n, void* stream);
+
 /* diagnostics: copies the sort control block of the last sort on `stream` */
 unsigned long long trtc_debug_sort_ctrl(void* host, unsigned long long bytes, void* stream);
 

@@ -1,0 +1,154 @@
+"""Batched segmented sort + exclusive scan (trtc_raw_segmented_sort_scan) against the oracle,
+segment by segment: every segment must equal a stable Sort_By_Key of that segment alone and
+the exclusive Plus scan (uint32 wrap-around) of its sorted values.  Bit-exact."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TC = {"uint32_t": 5, "int32_t": 4, "float": 8, "int64_t": 6, "uint64_t": 7}
+NP = {"uint32_t": np.uint32, "int32_t": np.int32, "float": np.float32, "int64_t": np.int64, "uint64_t": np.uint64}
+
+
+@pytest.fixture(scope="module")
+def N(cuda):
+    from thrustrtc_b200 import _native as N
+    L = N.lib
+    L.trtc_raw_segmented_workspace_bytes.restype = ctypes.c_ulonglong
+    L.trtc_raw_segmented_workspace_bytes.argtypes = [ctypes.c_int, ctypes.c_ulonglong, ctypes.c_ulonglong]
+    L.trtc_raw_segmented_sort_scan.restype = ctypes.c_int
+    L.trtc_raw_segmented_sort_scan.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + \
+        [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_void_p]
+    L.trtc_raw_segmented_autotune.restype = ctypes.c_int
+    L.trtc_raw_segmented_autotune.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong,
+                                              ctypes.c_ulonglong, ctypes.c_void_p]
+    return N
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def make_lengths(rng, nseg, median, sigma, hi):
+    z = rng.standard_normal(nseg)
+    lens = np.clip(np.round(np.exp(np.log(median) + sigma * z)), 1, hi).astype(np.int64)
+    return lens
+
+
+def keys_for(rng, name, n):
+    if name == "float":
+        x = (rng.standard_normal(n) * 100).astype(np.float32)
+        x[rng.integers(0, n, max(1, n // 50))] = -0.0
+        x[rng.integers(0, n, max(1, n // 50))] = 0.0
+        return x
+    info = np.iinfo(NP[name])
+    if rng.random() < 0.5:
+        return rng.integers(info.min, info.max, n, dtype=NP[name], endpoint=True)
+    return rng.integers(0, 50, n).astype(NP[name])  # many duplicates: stability matters
+
+
+def expected(keys, vals, off, desc):
+    ek, ev, es = keys.copy(), vals.copy(), np.zeros_like(vals)
+    for i in range(len(off) - 1):
+        a, b = off[i], off[i + 1]
+        if a == b:
+            continue
+        k, v = O.sort_by_key(keys[a:b], vals[a:b], desc)
+        ek[a:b], ev[a:b] = k, v
+        c = np.cumsum(v.astype(np.uint64)) & 0xFFFFFFFF
+        es[a:b] = np.concatenate([[0], c[:-1]]).astype(np.uint32)
+    return ek, ev, es
+
+
+def run(N, name, keys, vals, off, desc, stream=None):
+    import torch
+    n, nseg = len(keys), len(off) - 1
+    tk = torch.from_numpy(keys.view(np.int32) if keys.dtype.itemsize == 4 else keys.view(np.int64)).cuda()
+    tv = torch.from_numpy(vals.view(np.int32)).cuda()
+    ts = torch.full_like(tv, -1)
+    to = torch.from_numpy(off.astype(np.int64)).cuda()
+    wsb = N.lib.trtc_raw_segmented_workspace_bytes(TC[name], n, nseg)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    rc = N.lib.trtc_raw_segmented_sort_scan(TC[name], _p(tk), _p(tv), _p(ts), _p(to), nseg, n, _p(ws), wsb,
+                                            int(desc), stream)
+    assert rc == 0, N.last_error()
+    torch.cuda.synchronize()
+    return (tk.cpu().numpy().view(keys.dtype), tv.cpu().numpy().view(np.uint32), ts.cpu().numpy().view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["uint32_t", "int32_t", "float", "int64_t", "uint64_t"])
+@pytest.mark.parametrize("desc", [False, True])
+def test_segmented_matches_per_segment_sort_and_scan(N, name, desc):
+    rng = np.random.default_rng(7 + 3 * int(desc) + len(name))
+    lens = make_lengths(rng, 400, 64, 1.5, 20000)
+    lens[:5] = [0, 1, 2, 2048, 4097]     # empty, single, tile edges of both configurations
+    lens[5:8] = [4096, 4095, 12000]       # on-chip limit and a chunked segment
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    n = int(off[-1])
+    keys = keys_for(rng, name, n)
+    vals = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    gk, gv, gs = run(N, name, keys, vals, off, desc)
+    ek, ev, es = expected(keys, vals, off, desc)
+    assert gk.tobytes() == ek.tobytes()
+    assert np.array_equal(gv, ev)
+    assert np.array_equal(gs, es)
+
+
+def test_segmented_autotune_and_repeat(N):
+    import torch
+    rng = np.random.default_rng(11)
+    lens = make_lengths(rng, 3000, 256, 1.5, 1 << 20)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    n = int(off[-1])
+    to = torch.from_numpy(off).cuda()
+    chosen = N.lib.trtc_raw_segmented_autotune(5, _p(to), len(lens), n, None)
+    assert chosen in (8, 16), N.last_error()
+    keys = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    ek, ev, es = expected(keys, vals, off, False)
+    for _ in range(2):
+        gk, gv, gs = run(N, "uint32_t", keys, vals, off, False)
+        assert np.array_equal(gk, ek) and np.array_equal(gv, ev) and np.array_equal(gs, es)
+
+
+def test_segmented_cuda_graph_replay(N):
+    import torch
+    rng = np.random.default_rng(5)
+    lens = make_lengths(rng, 1000, 128, 1.5, 50000)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    n, nseg = int(off[-1]), len(lens)
+    keys = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    ek, ev, es = expected(keys, vals, off, False)
+    k0 = torch.from_numpy(keys.view(np.int32)).cuda()
+    v0 = torch.from_numpy(vals.view(np.int32)).cuda()
+    tk, tv, ts = torch.empty_like(k0), torch.empty_like(v0), torch.empty_like(v0)
+    to = torch.from_numpy(off).cuda()
+    wsb = N.lib.trtc_raw_segmented_workspace_bytes(5, n, nseg)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    s = torch.cuda.Stream()
+
+    def step():
+        tk.copy_(k0)
+        tv.copy_(v0)
+        rc = N.lib.trtc_raw_segmented_sort_scan(5, _p(tk), _p(tv), _p(ts), _p(to), nseg, n, _p(ws), wsb, 0,
+                                                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 0, N.last_error()
+
+    with torch.cuda.stream(s):
+        step()  # uncaptured first call sets the kernels up
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        step()
+    for _ in range(2):
+        ts.fill_(0)
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(tk.cpu().numpy().view(np.uint32), ek)
+        assert np.array_equal(tv.cpu().numpy().view(np.uint32), ev)
+        assert np.array_equal(ts.cpu().numpy().view(np.uint32), es)

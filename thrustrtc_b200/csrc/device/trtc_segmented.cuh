@@ -1,0 +1,293 @@
+// trtc_segmented.cuh -- batched segmented sort + scan: many independent segments of one
+// key/value array, each stably sorted by key and then exclusive-scanned (Plus) over its
+// sorted values, in one persistent launch fed by a device work queue.
+//
+// The reference sorts one vector per call (internal/radix_sort.cpp:165-553) and scans one
+// vector per call (internal/general_scan.cpp:8-88); a batch there is one call pair per
+// segment.  Here a CTA takes a segment id from the queue and sorts the whole segment itself:
+//   * small segments (<= 256 * ITEMS keys) are sorted on chip: four 8-bit LSD passes of
+//     warp multisplit ranking + shared-memory scatter, with the tile re-laid out so that
+//     every warp gets keys whatever the segment length; then the values are scanned and
+//     keys, values and scan are written once;
+//   * larger segments are sorted by the CTA in global memory: one read builds all digit
+//     histograms, then four chunked, stable scatter passes ping-pong between the segment and
+//     a temp array (mostly L2-resident for segments of up to a few MB), then a chunked
+//     scan with a running carry.
+// The queue lists the large segments first, so the longest work starts first.
+#pragma once
+#include "trtc_prelude.cuh"
+#include "trtc_radix.cuh"
+
+namespace trtc {
+
+struct SegCtrl {
+    unsigned long long next;        // work-queue cursor
+    unsigned long long front;       // large segments placed from the front
+    unsigned long long back;        // small segments placed from the back
+    unsigned long long pad;
+};
+
+// queue[] = large segments (len > tile) first, then small ones
+template <class OFF>
+__global__ void seg_queue_kernel(const OFF* __restrict__ off, unsigned long long nseg, unsigned long long tile,
+                                 uint32_t* __restrict__ queue, SegCtrl* ctrl) {
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < nseg;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long len = (unsigned long long)(off[i + 1] - off[i]);
+        if (len > tile) queue[atomicAdd(&ctrl->front, 1ull)] = (uint32_t)i;
+        else queue[nseg - 1 - atomicAdd(&ctrl->back, 1ull)] = (uint32_t)i;
+    }
+}
+
+// Ranks IT (<= ITEMS) warp-striped items per thread of a tile of `tile_n` keys: element
+// e = warp*32*IT + i*32 + lane.  On return pos[i] is the item's position in the digit-sorted
+// tile (stable), s_cnt[d] / s_start[d] the tile's digit counts and exclusive starts.
+template <class K, bool DESC, int ITEMS>
+__device__ inline void seg_rank_tile(const typename RadixKey<K>::B (&keys)[ITEMS], uint32_t (&pos)[ITEMS], int IT,
+                                     uint32_t tile_n, uint32_t sel, bool hi, uint32_t* s_whist, uint32_t* s_cnt,
+                                     uint32_t* s_start, uint32_t* s_wsum) {
+    constexpr int WARPS = 8;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < WARPS * 256; i += 256) s_whist[i] = 0;
+    __syncthreads();
+    uint32_t* wh = s_whist + warp * 256;
+    const uint32_t ltm = lanemask_lt();
+    const uint32_t wbase = warp * 32u * (uint32_t)IT;
+    uint32_t info[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        pos[i] = 0;
+        info[i] = 0;
+        if (i >= IT || wbase + (uint32_t)i * 32u >= tile_n) continue;  // warp-uniform
+        const bool valid = wbase + (uint32_t)i * 32u + lane < tile_n;
+        const uint32_t d = radix_digit_sel<K, DESC>(keys[i], sel, hi);
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const bool set = (d >> b) & 1u;
+            const uint32_t bb = __ballot_sync(0xffffffffu, set);
+            peers &= set ? bb : ~bb;
+        }
+        const uint32_t leader = 31u - __clz(peers);
+        info[i] = (uint32_t)__popc(peers & ltm) | (leader << 8);
+        if (valid && lane == leader) pos[i] = atomicAdd(&wh[d], (uint32_t)__popc(peers));
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        if (i >= IT || wbase + (uint32_t)i * 32u >= tile_n) continue;
+        pos[i] = __shfl_sync(0xffffffffu, pos[i], (int)(info[i] >> 8)) + (info[i] & 0xFFu);
+    }
+    __syncthreads();
+    const uint32_t d = threadIdx.x;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; w++) cnt += s_whist[w * 256 + d];
+    const uint32_t start = block_excl_scan_256<256>(cnt, s_wsum);
+    s_cnt[d] = cnt;
+    s_start[d] = start;
+    uint32_t run = start;
+#pragma unroll
+    for (int w = 0; w < WARPS; w++) {
+        const uint32_t c = s_whist[w * 256 + d];
+        s_whist[w * 256 + d] = run;
+        run += c;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        if (i >= IT || wbase + (uint32_t)i * 32u + lane >= tile_n) continue;
+        pos[i] += wh[radix_digit_sel<K, DESC>(keys[i], sel, hi)];
+    }
+}
+
+// exclusive Plus scan of s_v[0..len) into s_o (256 threads, len <= 256 * ITEMS), carry-in c
+template <class V, int ITEMS>
+__device__ inline V seg_block_excl_scan(const V* s_v, V* s_o, uint32_t len, V carry, V* s_part) {
+    const uint32_t t = threadIdx.x;
+    const uint32_t per = (len + 255u) / 256u;  // consecutive elements per thread
+    const uint32_t b = t * per;
+    V sum = V();
+    for (uint32_t k = 0; k < per; k++)
+        if (b + k < len) sum += s_v[b + k];
+    // block exclusive scan of the thread sums (values of any width: two warp levels)
+    const uint32_t lane = t & 31u, w = t >> 5;
+    V x = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const V y = shfl_up_any(x, d);
+        if (lane >= (uint32_t)d) x += y;
+    }
+    if (lane == 31) s_part[w] = x;
+    __syncthreads();
+    V pre = carry;
+    for (uint32_t i = 0; i < w; i++) pre += s_part[i];
+    V total = carry;
+    for (int i = 0; i < 8; i++) total += s_part[i];
+    V run = pre + x - sum;
+    for (uint32_t k = 0; k < per; k++)
+        if (b + k < len) { s_o[b + k] = run; run += s_v[b + k]; }
+    __syncthreads();
+    return total;
+}
+
+template <class K, class V, int ITEMS>
+constexpr size_t seg_sort_scan_smem() {
+    return (size_t)256 * ITEMS * (2 * sizeof(V) + sizeof(typename RadixKey<K>::B)) + 8 * 256 * 4;
+}
+
+// One persistent launch over the whole batch.  keys/vals: the concatenated segments (sorted
+// in place); scan: receives the exclusive scans; tk/tv: temp arrays of n elements (large
+// segments only).
+template <class K, class V, class OFF, bool DESC, int ITEMS>
+__global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey<K>::B* __restrict__ keys,
+                                                                V* __restrict__ vals, V* __restrict__ scan,
+                                                                typename RadixKey<K>::B* __restrict__ tk,
+                                                                V* __restrict__ tv, const OFF* __restrict__ off,
+                                                                const uint32_t* __restrict__ queue,
+                                                                unsigned long long nseg, SegCtrl* ctrl) {
+    typedef typename RadixKey<K>::B KB;
+    constexpr int TILE = 256 * ITEMS;
+    constexpr int D = RadixKey<K>::DIGITS;
+    extern __shared__ __align__(16) unsigned char seg_smem[];  // seg_sort_scan_smem<K, V, ITEMS>() bytes
+    V* s_v = reinterpret_cast<V*>(seg_smem);
+    V* s_o = s_v + TILE;
+    KB* s_k = reinterpret_cast<KB*>(s_o + TILE);
+    uint32_t* s_whist = reinterpret_cast<uint32_t*>(s_k + TILE);
+    __shared__ uint32_t s_cnt[256], s_start[256], s_run[256];
+    __shared__ uint32_t s_hist[D][256];
+    __shared__ uint32_t s_wsum[8];
+    __shared__ V s_part[8];
+    __shared__ unsigned long long s_item;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctrl->next, 1ull);
+        __syncthreads();
+        const unsigned long long item = s_item;
+        if (item >= nseg) return;
+        const uint32_t sid = queue[item];
+        const unsigned long long base = (unsigned long long)off[sid];
+        const uint32_t len = (uint32_t)((unsigned long long)off[sid + 1] - base);
+        if (len == 0) continue;
+        KB* gk = keys + base;
+        V* gv = vals + base;
+        V* gs = scan + base;
+
+        if (len <= (uint32_t)TILE) {
+            // ---------------- on-chip sort of a small segment
+            const int IT = (int)((len + 255u) / 256u);
+            const uint32_t wbase = warp * 32u * (uint32_t)IT;
+            KB k[ITEMS];
+            V v[ITEMS];
+            uint32_t pos[ITEMS];
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t e = wbase + (uint32_t)i * 32u + lane;
+                if (i < IT && e < len) { k[i] = gk[e]; v[i] = gv[e]; }
+                else { k[i] = KB(0); v[i] = V(); }
+            }
+            for (int p = 0; p < D; p++) {
+                const uint32_t sel = 0x4440u | (uint32_t)(p & 3);
+                seg_rank_tile<K, DESC, ITEMS>(k, pos, IT, len, sel, p >= 4, s_whist, s_cnt, s_start, s_wsum);
+#pragma unroll
+                for (int i = 0; i < ITEMS; i++) {
+                    const uint32_t e = wbase + (uint32_t)i * 32u + lane;
+                    if (i < IT && e < len) { s_k[pos[i]] = k[i]; s_v[pos[i]] = v[i]; }
+                }
+                __syncthreads();
+                if (p + 1 < D) {
+#pragma unroll
+                    for (int i = 0; i < ITEMS; i++) {
+                        const uint32_t e = wbase + (uint32_t)i * 32u + lane;
+                        if (i < IT && e < len) { k[i] = s_k[e]; v[i] = s_v[e]; }
+                    }
+                }
+                __syncthreads();
+            }
+            // s_k / s_v hold the sorted segment; exclusive scan of the values into s_o
+            seg_block_excl_scan<V, ITEMS>(s_v, s_o, len, V(), s_part);
+            for (uint32_t e = threadIdx.x; e < len; e += 256) {
+                gk[e] = s_k[e];
+                gv[e] = s_v[e];
+                gs[e] = s_o[e];
+            }
+            continue;
+        }
+
+        // ---------------- large segment: CTA-level LSD passes through global memory
+        for (int i = threadIdx.x; i < D * 256; i += 256) (&s_hist[0][0])[i] = 0;
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < len; e += 256) {
+            typename RadixKey<K>::U u = RadixKey<K>::ordered(gk[e]);
+            if (DESC) u = ~u;
+#pragma unroll
+            for (int p = 0; p < D; p++) {
+                const uint32_t w = (p < 4) ? (uint32_t)u : (uint32_t)((unsigned long long)u >> 32);
+                atomicAdd(&s_hist[p][__byte_perm(w, 0u, 0x4440u | (uint32_t)(p & 3))], 1u);
+            }
+        }
+        __syncthreads();
+        KB* sk = gk;
+        V* sv = gv;
+        KB* dk = tk + base;
+        V* dv = tv + base;
+        for (int p = 0; p < D; p++) {
+            const uint32_t sel = 0x4440u | (uint32_t)(p & 3);
+            const bool hi = p >= 4;
+            {
+                const uint32_t c = s_hist[p][threadIdx.x];
+                s_run[threadIdx.x] = block_excl_scan_256<256>(c, s_wsum);
+            }
+            __syncthreads();
+            for (uint32_t cb = 0; cb < len; cb += TILE) {
+                const uint32_t cn = min((uint32_t)TILE, len - cb);
+                const uint32_t wbase = warp * 32u * ITEMS;
+                KB k[ITEMS];
+                V v[ITEMS];
+                uint32_t pos[ITEMS];
+#pragma unroll
+                for (int i = 0; i < ITEMS; i++) {
+                    const uint32_t e = wbase + (uint32_t)i * 32u + lane;
+                    if (e < cn) { k[i] = sk[cb + e]; v[i] = sv[cb + e]; }
+                    else { k[i] = KB(0); v[i] = V(); }
+                }
+                seg_rank_tile<K, DESC, ITEMS>(k, pos, ITEMS, cn, sel, hi, s_whist, s_cnt, s_start, s_wsum);
+#pragma unroll
+                for (int i = 0; i < ITEMS; i++) {
+                    const uint32_t e = wbase + (uint32_t)i * 32u + lane;
+                    if (e < cn) { s_k[pos[i]] = k[i]; s_v[pos[i]] = v[i]; }
+                }
+                __syncthreads();
+                for (uint32_t e = threadIdx.x; e < cn; e += 256) {
+                    const KB key = s_k[e];
+                    const uint32_t d = radix_digit_sel<K, DESC>(key, sel, hi);
+                    const uint32_t dst = s_run[d] + (e - s_start[d]);
+                    dk[dst] = key;
+                    dv[dst] = s_v[e];
+                }
+                __syncthreads();
+                s_run[threadIdx.x] += s_cnt[threadIdx.x];
+                __syncthreads();
+            }
+            KB* t1 = sk; sk = dk; dk = t1;
+            V* t2 = sv; sv = dv; dv = t2;
+        }
+        // after D passes the segment is in sk/sv (the caller's arrays when D is even);
+        // chunked exclusive scan with a running carry, writing keys and values back if needed
+        V carry = V();
+        for (uint32_t cb = 0; cb < len; cb += TILE) {
+            const uint32_t cn = min((uint32_t)TILE, len - cb);
+            for (uint32_t e = threadIdx.x; e < cn; e += 256) {
+                s_v[e] = sv[cb + e];
+                if (sk != gk) { gk[cb + e] = sk[cb + e]; gv[cb + e] = s_v[e]; }
+            }
+            __syncthreads();
+            carry = seg_block_excl_scan<V, ITEMS>(s_v, s_o, cn, carry, s_part);
+            for (uint32_t e = threadIdx.x; e < cn; e += 256) gs[cb + e] = s_o[e];
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace trtc

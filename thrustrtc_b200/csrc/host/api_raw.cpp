@@ -104,4 +104,22 @@ unsigned long long trtc_raw_unique_copy(int tc, const void* in, void* out, unsig
     return compact_raw(tc, COMPACT_UNIQUE, in, out, (size_t)n, nullptr, S(stream), &c) ? c : ~0ull;
 }
 
+unsigned long long trtc_raw_segmented_workspace_bytes(int key_type, unsigned long long n, unsigned long long nseg) {
+    return segmented_workspace_bytes(key_type, (size_t)n, (size_t)nseg);
+}
+
+int trtc_raw_segmented_sort_scan(int key_type, void* keys, void* values, void* scan_out,
+                                 const unsigned long long* offsets, unsigned long long nseg, unsigned long long n,
+                                 void* workspace, unsigned long long workspace_bytes, int descending, void* stream) {
+    if (!ensure_device()) return -1;
+    return segmented_sort_scan_raw(key_type, keys, values, scan_out, offsets, (size_t)nseg, (size_t)n, workspace,
+                                   (size_t)workspace_bytes, descending != 0, S(stream)) ? 0 : -1;
+}
+
+int trtc_raw_segmented_autotune(int key_type, const unsigned long long* offsets, unsigned long long nseg,
+                                unsigned long long n, void* stream) {
+    int chosen = 0;
+    return segmented_autotune(key_type, offsets, (size_t)nseg, (size_t)n, S(stream), &chosen) ? chosen : -1;
+}
+
 }  // extern "C"

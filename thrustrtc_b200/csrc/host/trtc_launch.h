@@ -29,4 +29,11 @@ bool scan_by_key_raw(int key_tc, int val_tc, int mode, const void* keys, const v
 bool compact_raw(int tc, int mode, const void* in, void* out, size_t n, const void* value, cudaStream_t s,
                  unsigned long long* count);
 
+// batched segmented sort + exclusive scan (launch_segmented.cu); 4-byte values
+size_t segmented_workspace_bytes(int tc, size_t n, size_t nseg);
+int segmented_tuned_items(int tc);
+bool segmented_sort_scan_raw(int tc, void* keys, void* vals, void* scan, const unsigned long long* off, size_t nseg,
+                             size_t n, void* ws, size_t ws_bytes, bool desc, cudaStream_t s);
+bool segmented_autotune(int tc, const unsigned long long* off, size_t nseg, size_t n, cudaStream_t s, int* chosen);
+
 }  // namespace trtc_host
