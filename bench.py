@@ -55,6 +55,9 @@ WORKLOADS = {
                         "Gkeys/s sort 2^28 u32 pairs, % HBM roofline", "Gkeys/s"),
     "inclusive_scan_i32": (1 << 28, "scan_kernel", 8, 8, "GB/s inclusive scan 2^28 i32, % HBM roofline", "GB/s"),
     "reduce_f32": (1 << 28, "reduce_kernel", 4, 4, "GB/s reduce 2^28 f32, % HBM roofline", "GB/s"),
+    # batched form: 100,000 lognormal segments (~2^26 pairs), each sorted then exclusive-scanned
+    "segmented_c4": (100_000, "seg_sort_scan_kernel", 20, 20,
+                     "Gkeys/s batched segmented sort+scan, 100k lognormal segments", "Gkeys/s"),
 }
 
 M64 = (1 << 64) - 1
@@ -181,6 +184,23 @@ def cpu_run(workload, sample_n, threads):
     """One timed oracle run on the host over the first `sample_n` units; returns (seconds,
     threads used): the pair sort runs on `threads` threads, the scan and reduce on one."""
     from oracle import oracle as O
+    if workload == "segmented_c4":
+        # sample_n segments spread over the batch, one oracle sort + scan per segment,
+        # segments spread over `threads` host threads
+        import concurrent.futures as cf
+        keys, vals, off = gen_segmented(WORKLOADS["segmented_c4"][0])
+        idx = np.linspace(0, len(off) - 2, sample_n).astype(np.int64)
+
+        def one(i):
+            a, b = int(off[i]), int(off[i + 1])
+            kk, vv = O.sort_pairs32(keys[a:b], vals[a:b], False, 1)
+            np.cumsum(vv, dtype=np.uint32)
+            return b - a
+
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(threads) as ex:
+            pairs = sum(ex.map(one, idx))
+        return time.perf_counter() - t0, threads, pairs
     x, v = gen_inputs(workload, sample_n)
     t0 = time.perf_counter()
     if workload == "sort_by_key_u32":
@@ -189,12 +209,12 @@ def cpu_run(workload, sample_n, threads):
         O.scan(x)
     else:
         O.reduce(x)
-    return time.perf_counter() - t0, (threads if workload == "sort_by_key_u32" else 1)
+    return time.perf_counter() - t0, (threads if workload == "sort_by_key_u32" else 1), sample_n
 
 
 def units_per_s_to_metric(workload, units, seconds):
     """Throughput in the metric's unit: Gkeys/s for sorts, GB/s of algorithmic bytes otherwise."""
-    if workload == "sort_by_key_u32":
+    if workload in ("sort_by_key_u32", "segmented_c4"):
         return units / seconds / 1e9
     return units * WORKLOADS[workload][3] / seconds / 1e9
 
@@ -207,17 +227,22 @@ def run_reference(args):
     wl = args.workload
     n, _, _, _, metric, unit = WORKLOADS[wl]
     threads = cpu_threads()
-    sample = args.cpu_sample or (1 << 25 if wl == "sort_by_key_u32" else 1 << 27)
+    sample = args.cpu_sample or {"sort_by_key_u32": 1 << 25, "segmented_c4": 20000}.get(wl, 1 << 27)
     from oracle import oracle as O
     O.build()
     for _ in range(args.warmup):
         cpu_run(wl, sample, threads)
     ts = [cpu_run(wl, sample, threads) for _ in range(args.steps)]
-    tot = sum(t for t, _ in ts)
+    tot = sum(t for t, _, _ in ts)
     threads = ts[0][1]
-    value = units_per_s_to_metric(wl, sample * args.steps, tot)
-    desc = ("first %d units of the %s workload (n=%d); oracle restatement of the reference's "
-            "algorithm, %d host threads" % (sample, wl, n, threads))
+    units = sum(u for _, _, u in ts)
+    value = units_per_s_to_metric(wl, units, tot)
+    if wl == "segmented_c4":
+        desc = ("%d of the %d segments per step, spread over the batch; oracle sort + exclusive scan per "
+                "segment, %d host threads" % (sample, n, threads))
+    else:
+        desc = ("first %d units of the %s workload (n=%d); oracle restatement of the reference's "
+                "algorithm, %d host threads" % (sample, wl, n, threads))
     line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": _dtype(wl),
@@ -231,7 +256,7 @@ def run_reference(args):
 
 
 def _dtype(wl):
-    return {"sort_by_key_u32": "u32", "inclusive_scan_i32": "int32", "reduce_f32": "f32"}[wl]
+    return {"sort_by_key_u32": "u32", "inclusive_scan_i32": "int32", "reduce_f32": "f32", "segmented_c4": "u32"}[wl]
 
 
 def _config(wl, n, world):
@@ -240,6 +265,9 @@ def _config(wl, n, world):
     if wl == "sort_by_key_u32":
         base.update({"keys": "uint32 uniform over 32 bits", "values": "uint32 = index", "order": "ascending, stable",
                      "step": "restore the unsorted pairs from a pristine copy (untimed), then one sort (timed)"})
+    elif wl == "segmented_c4":
+        base = {"workload": wl, "segments": n, "lengths": "lognormal median 256 sigma 1.5 clipped [1, 2^20]",
+                "keys": "uint32 uniform", "values": "uint32 = index", "parallelism": "replicas x%d" % world}
     elif wl == "inclusive_scan_i32":
         base.update({"values": "int32 uniform in [-1000, 1000]", "op": "Plus"})
     else:
@@ -376,7 +404,7 @@ def run_ours(args):
         threads = cpu_threads()
         sample = args.cpu_sample or (1 << 25 if wl == "sort_by_key_u32" else 1 << 27)
         sample = min(sample, n)
-        secs, threads = cpu_run(wl, sample, threads)
+        secs, threads, _ = cpu_run(wl, sample, threads)
         cpu = {"value": units_per_s_to_metric(wl, sample, secs), "unit": unit, "cores": threads, "kind": "port",
                "sample": "first %d units of the same workload, oracle host restatement, %d threads" % (sample, threads)}
 
@@ -489,6 +517,243 @@ def _e2e(args, wl, n, keys_h, vals_h, world, max_over_ranks, barrier):
                      "reduce_f32": "n_reduce"}[wl]}
 
 
+# ---------------------------------------------------------------- batched segmented form
+def segment_lengths(nseg, seed=0):
+    """Lognormal lengths, median 256, sigma 1.5, clipped to [1, 2^20] (Box-Muller on SplitMix64)."""
+    h = splitmix64(seed, 1, 2 * nseg)
+    u1 = ((h[0::2] >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+    u2 = ((h[1::2] >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+    z = np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+    return np.clip(np.round(np.exp(np.log(256.0) + 1.5 * z)), 1, 1 << 20).astype(np.int64)
+
+
+_SEG_CACHE = {}
+
+
+def gen_segmented(nseg):
+    if nseg in _SEG_CACHE:
+        return _SEG_CACHE[nseg]
+    _SEG_CACHE[nseg] = _gen_segmented(nseg)
+    return _SEG_CACHE[nseg]
+
+
+def _gen_segmented(nseg):
+    lens = segment_lengths(nseg)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    n = int(off[-1])
+    keys = (splitmix64(0, 0, n) >> np.uint64(32)).astype(np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    return keys, vals, off
+
+
+def _seg_sigs(L):
+    L.trtc_raw_segmented_workspace_bytes.restype = ctypes.c_ulonglong
+    L.trtc_raw_segmented_workspace_bytes.argtypes = [ctypes.c_int, ctypes.c_ulonglong, ctypes.c_ulonglong]
+    L.trtc_raw_segmented_sort_scan.restype = ctypes.c_int
+    L.trtc_raw_segmented_sort_scan.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + \
+        [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_void_p]
+    L.trtc_raw_segmented_autotune.restype = ctypes.c_int
+    L.trtc_raw_segmented_autotune.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong,
+                                              ctypes.c_ulonglong, ctypes.c_void_p]
+
+
+def run_segmented(args):
+    """100,000 uneven segments sorted and exclusive-scanned in one persistent launch, replayed
+    from a CUDA graph; beside it one plain sort + scan call pair per segment on a sample."""
+    import torch
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: a CUDA device is required (there is no CPU path)")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    import thrustrtc_b200 as trtc
+    from thrustrtc_b200 import _native as N
+    trtc.init()
+    L = N.lib
+    _seg_sigs(L)
+    nseg = args.n or WORKLOADS["segmented_c4"][0]
+    keys_h, vals_h, off_h = gen_segmented(nseg)
+    n = len(keys_h)
+    k0 = torch.from_numpy(keys_h.view(np.int32)).to(dev)
+    v0 = torch.from_numpy(vals_h.view(np.int32)).to(dev)
+    k, v, sc = torch.empty_like(k0), torch.empty_like(v0), torch.empty_like(v0)
+    off = torch.from_numpy(off_h).to(dev)
+    wsb = L.trtc_raw_segmented_workspace_bytes(5, n, nseg)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    items = L.trtc_raw_segmented_autotune(5, P(off), nseg, n, None)
+    if items < 0:
+        raise RuntimeError(N.last_error())
+    stream = torch.cuda.Stream(device=dev)
+
+    def call():
+        rc = L.trtc_raw_segmented_sort_scan(5, P(k), P(v), P(sc), P(off), nseg, n, P(ws), wsb, 0,
+                                            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise RuntimeError(N.last_error())
+
+    with torch.cuda.stream(stream):
+        k.copy_(k0); v.copy_(v0)
+        call()  # uncaptured first call: kernel set-up
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        call()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            k.copy_(k0); v.copy_(v0)
+            g.replay()
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(dev)
+    with sampler, torch.cuda.stream(stream):
+        barrier()
+        for i in range(args.steps):
+            k.copy_(k0); v.copy_(v0)  # restore (untimed)
+            ev[i][0].record()
+            g.replay()
+            ev[i][1].record()
+        barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    tot_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    value = n * world * args.steps / (tot_ms / 1e3) / 1e9
+
+    # correctness of the last replay: per-segment sortedness, stability, scan (size-independent
+    # properties over the whole batch, on the device)
+    seg_id = torch.repeat_interleave(torch.arange(nseg, device=dev), off[1:] - off[:-1])
+    ku = k.to(torch.int64) & 0xFFFFFFFF
+    same = seg_id[1:] == seg_id[:-1]
+    if not bool(((ku[1:] >= ku[:-1]) | ~same).all()):
+        raise RuntimeError("segmented check failed: a segment is not sorted")
+    perm = v.to(torch.int64) & 0xFFFFFFFF
+    if not bool((k0[perm] == k).all()) or not bool((seg_id[perm] == seg_id).all()):
+        raise RuntimeError("segmented check failed: values are not the keys' permutation within segments")
+    eq = same & (ku[1:] == ku[:-1])
+    if not bool((perm[1:][eq] > perm[:-1][eq]).all()):
+        raise RuntimeError("segmented check failed: not stable")
+    cs = torch.cumsum(perm, 0)
+    seg_start_cs = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), cs])[off[:-1]]
+    excl = (cs - perm - seg_start_cs[seg_id]) & 0xFFFFFFFF
+    if not bool((excl == (sc.to(torch.int64) & 0xFFFFFFFF)).all()):
+        raise RuntimeError("segmented check failed: exclusive scan")
+
+    # dominant kernel time from uncaptured calls with per-launch events
+    N.timing_enable(True)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            k.copy_(k0); v.copy_(v0)
+            call()
+    recs = N.timing_records()
+    N.timing_enable(False)
+    kt = [ms for name, ms in recs if name == "seg_sort_scan_kernel"]
+    peak, peak_src = measured_peak()
+    per_launch_ms = statistics.mean(kt) if kt else None
+    achieved = 20.0 * n / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else None
+
+    # plain path: one trtc_raw_sort_by_key + one exclusive trtc_raw_scan per segment, on a
+    # sample of segments spread over the batch, extrapolated by segment count
+    plain = None
+    if not args.no_plain:
+        sample = min(nseg, 1000)
+        idx = np.linspace(0, nseg - 1, sample).astype(np.int64)
+        zero = np.zeros(1, np.uint32)
+        torch.cuda.synchronize()
+        k.copy_(k0); v.copy_(v0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in idx:
+            a, b = int(off_h[i]), int(off_h[i + 1])
+            if L.trtc_raw_sort_by_key(5, ctypes.c_void_p(k.data_ptr() + 4 * a), ctypes.c_void_p(v.data_ptr() + 4 * a),
+                                      4, b - a, 0, None) != 0:
+                raise RuntimeError(N.last_error())
+            if L.trtc_raw_scan(5, 0, 1, ctypes.c_void_p(v.data_ptr() + 4 * a), ctypes.c_void_p(sc.data_ptr() + 4 * a),
+                               b - a, zero.ctypes.data_as(ctypes.c_void_p), None) != 0:
+                raise RuntimeError(N.last_error())
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        pairs = int((off_h[idx + 1] - off_h[idx]).sum())
+        plain = {"value": pairs / secs / 1e9, "unit": "Gkeys/s", "sample_segments": int(sample),
+                 "ms_per_segment": secs / sample * 1e3,
+                 "ms_all_segments_extrapolated": secs / sample * nseg * 1e3,
+                 "path": "trtc_raw_sort_by_key + trtc_raw_scan (exclusive) per segment"}
+
+    e2e = None
+    if not args.no_e2e:
+        kp = torch.from_numpy(keys_h.view(np.int32)).pin_memory()
+        vp_ = torch.from_numpy(vals_h.view(np.int32)).pin_memory()
+        op = torch.from_numpy(off_h).pin_memory()
+        ko, vo, so = torch.empty_like(kp).pin_memory(), torch.empty_like(vp_).pin_memory(), torch.empty_like(vp_).pin_memory()
+        steps = max(1, min(args.steps, args.e2e_steps))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            k.copy_(kp, non_blocking=True); v.copy_(vp_, non_blocking=True); off.copy_(op, non_blocking=True)
+            call()
+            ko.copy_(k, non_blocking=True); vo.copy_(v, non_blocking=True); so.copy_(sc, non_blocking=True)
+        barrier()
+        secs = time.perf_counter() - t0
+        e2e = {"value": n * world * steps / secs / 1e9, "unit": "Gkeys/s", "h2d_bytes_per_step": 8 * n + 8 * (nseg + 1),
+               "d2h_bytes_per_step": 12 * n, "steps": steps, "ms_per_step": secs / steps * 1e3,
+               "path": "pinned host -> device, trtc_raw_segmented_sort_scan, device -> pinned host"}
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu:
+        from oracle import oracle as O
+        sample = min(nseg, 5000)
+        idx = np.linspace(0, nseg - 1, sample).astype(np.int64)
+        t0 = time.perf_counter()
+        pairs = 0
+        for i in idx:
+            a, b = int(off_h[i]), int(off_h[i + 1])
+            kk, vv = O.sort_pairs32(keys_h[a:b], vals_h[a:b], False, 1)
+            np.cumsum(vv, dtype=np.uint32)
+            pairs += b - a
+        secs = time.perf_counter() - t0
+        cpu = {"value": pairs / secs / 1e9, "unit": "Gkeys/s", "cores": 1, "kind": "port",
+               "sample": "%d of the %d segments (%d pairs), oracle sort + scan per segment, 1 thread" %
+                         (sample, nseg, pairs)}
+
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        line = {"metric": WORKLOADS["segmented_c4"][4], "value": value, "unit": "Gkeys/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                "data": "synthetic (SplitMix64 seed 0, generated on the host)",
+                "config": {"workload": "segmented_c4", "segments": nseg, "n": n,
+                           "lengths": "lognormal median 256 sigma 1.5 clipped [1, 2^20]",
+                           "keys": "uint32 uniform", "values": "uint32 = index",
+                           "op": "stable sort by key per segment, then exclusive Plus scan of its values",
+                           "launch": "1 persistent launch from a device work queue (+1 queue kernel), CUDA graph replay",
+                           "autotuned_items_per_thread": items, "parallelism": "replicas x%d" % world,
+                           "l2": "inputs (%d MiB) exceed the 126 MB L2" % (8 * n >> 20)},
+                "roofline": {"bound": "hbm", "kernel": "seg_sort_scan_kernel", "achieved": achieved, "peak": peak,
+                             "peak_source": peak_src, "unit": "GB/s",
+                             "frac": (achieved / peak) if achieved else None, "traffic": None,
+                             "algorithmic_bytes_per_unit": 20, "launch_ms": per_launch_ms},
+                "plain_per_segment": plain, "cpu_baseline": cpu, "e2e": e2e, "clocks": sampler.summary(),
+                "gpu_launches": 2 * args.steps, "step_ms": [round(x, 4) for x in step_ms]}
+        print(json.dumps(line), flush=True)
+    del g
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -502,6 +767,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--allow-short-warmup", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="segmented_c4: skip the per-segment plain calls")
     args = ap.parse_args()
     _, world, _ = dist_env()
     if args.gpus != world and not (args.gpus == 1 and world == 1):
@@ -509,6 +775,8 @@ def main():
             raise SystemExit("bench.py: for --gpus N > 1 launch one process per GPU with torchrun")
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "segmented_c4":
+        return run_segmented(args)
     return run_ours(args)
 
 
