@@ -23,7 +23,7 @@ def exported():
     return set(line.split()[-1] for line in out.splitlines() if line.strip())
 
 
-@pytest.mark.parametrize("header", ["thrustrtc_b200.h", "trtc_raw.h"])
+@pytest.mark.parametrize("header", ["thrustrtc_b200.h", "trtc_raw.h", "trtc_server.h"])
 def test_every_declared_symbol_is_exported(header, exported):
     names = _declared(header)
     assert names, header

@@ -20,6 +20,17 @@
 
 namespace trtc {
 
+// One segment given by its own arrays (list mode, used by the request server): keys k and
+// 4-byte values v sorted in place, out = exclusive scan of the sorted values (or nullptr),
+// n elements, toff = the segment's offset in the temp arrays.
+struct SegItem {
+    void* k;
+    void* v;
+    void* out;
+    unsigned long long n;
+    unsigned long long toff;
+};
+
 struct SegCtrl {
     unsigned long long next;        // work-queue cursor
     unsigned long long front;       // large segments placed from the front
@@ -144,7 +155,8 @@ __global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey
                                                                 typename RadixKey<K>::B* __restrict__ tk,
                                                                 V* __restrict__ tv, const OFF* __restrict__ off,
                                                                 const uint32_t* __restrict__ queue,
-                                                                unsigned long long nseg, SegCtrl* ctrl) {
+                                                                unsigned long long nseg, SegCtrl* ctrl,
+                                                                const SegItem* __restrict__ items) {
     typedef typename RadixKey<K>::B KB;
     constexpr int TILE = 256 * ITEMS;
     constexpr int D = RadixKey<K>::DIGITS;
@@ -166,13 +178,27 @@ __global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey
         __syncthreads();
         const unsigned long long item = s_item;
         if (item >= nseg) return;
-        const uint32_t sid = queue[item];
-        const unsigned long long base = (unsigned long long)off[sid];
-        const uint32_t len = (uint32_t)((unsigned long long)off[sid + 1] - base);
+        KB* gk;
+        V* gv;
+        V* gs;
+        uint32_t len;
+        unsigned long long base;
+        if (items) {  // list mode: segments in queue order, each with its own arrays
+            const SegItem it = items[item];
+            gk = reinterpret_cast<KB*>(it.k);
+            gv = reinterpret_cast<V*>(it.v);
+            gs = reinterpret_cast<V*>(it.out);
+            len = (uint32_t)it.n;
+            base = it.toff;
+        } else {
+            const uint32_t sid = queue[item];
+            base = (unsigned long long)off[sid];
+            len = (uint32_t)((unsigned long long)off[sid + 1] - base);
+            gk = keys + base;
+            gv = vals + base;
+            gs = scan + base;
+        }
         if (len == 0) continue;
-        KB* gk = keys + base;
-        V* gv = vals + base;
-        V* gs = scan + base;
 
         if (len <= (uint32_t)TILE) {
             // ---------------- on-chip sort of a small segment
@@ -206,11 +232,11 @@ __global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey
                 __syncthreads();
             }
             // s_k / s_v hold the sorted segment; exclusive scan of the values into s_o
-            seg_block_excl_scan<V, ITEMS>(s_v, s_o, len, V(), s_part);
+            if (gs) seg_block_excl_scan<V, ITEMS>(s_v, s_o, len, V(), s_part);
             for (uint32_t e = threadIdx.x; e < len; e += 256) {
                 gk[e] = s_k[e];
                 gv[e] = s_v[e];
-                gs[e] = s_o[e];
+                if (gs) gs[e] = s_o[e];
             }
             continue;
         }
@@ -283,9 +309,71 @@ __global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey
                 if (sk != gk) { gk[cb + e] = sk[cb + e]; gv[cb + e] = s_v[e]; }
             }
             __syncthreads();
-            carry = seg_block_excl_scan<V, ITEMS>(s_v, s_o, cn, carry, s_part);
-            for (uint32_t e = threadIdx.x; e < cn; e += 256) gs[cb + e] = s_o[e];
+            if (gs) {
+                carry = seg_block_excl_scan<V, ITEMS>(s_v, s_o, cn, carry, s_part);
+                for (uint32_t e = threadIdx.x; e < cn; e += 256) gs[cb + e] = s_o[e];
+            }
             __syncthreads();
+        }
+    }
+}
+
+// Exclusive Plus scans of many segments (list mode): a persistent CTA takes one segment at
+// a time and scans it in chunks of 256 * ITEMS with a running carry.
+template <class T, int ITEMS>
+__global__ void __launch_bounds__(256) seg_scan_list_kernel(const SegItem* __restrict__ items, unsigned long long nseg,
+                                                            SegCtrl* ctrl) {
+    constexpr int TILE = 256 * ITEMS;
+    __shared__ __align__(16) T s_v[TILE];
+    __shared__ __align__(16) T s_o[TILE];
+    __shared__ T s_part[8];
+    __shared__ unsigned long long s_item;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctrl->next, 1ull);
+        __syncthreads();
+        const unsigned long long item = s_item;
+        if (item >= nseg) return;
+        const SegItem it = items[item];
+        const T* in = reinterpret_cast<const T*>(it.k);
+        T* out = reinterpret_cast<T*>(it.out);
+        T carry = T();
+        for (unsigned long long cb = 0; cb < it.n; cb += TILE) {
+            const uint32_t cn = (uint32_t)min((unsigned long long)TILE, it.n - cb);
+            for (uint32_t e = threadIdx.x; e < cn; e += 256) s_v[e] = in[cb + e];
+            __syncthreads();
+            carry = seg_block_excl_scan<T, ITEMS>(s_v, s_o, cn, carry, s_part);
+            for (uint32_t e = threadIdx.x; e < cn; e += 256) out[cb + e] = s_o[e];
+            __syncthreads();
+        }
+    }
+}
+
+// Plus reductions of many segments (list mode); the result of segment i goes to
+// *(T*)items[i].out.
+template <class T>
+__global__ void __launch_bounds__(256) seg_reduce_list_kernel(const SegItem* __restrict__ items, unsigned long long nseg,
+                                                              SegCtrl* ctrl) {
+    __shared__ T s_w[8];
+    __shared__ unsigned long long s_item;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctrl->next, 1ull);
+        __syncthreads();
+        const unsigned long long item = s_item;
+        if (item >= nseg) return;
+        const SegItem it = items[item];
+        const T* in = reinterpret_cast<const T*>(it.k);
+        T a = T();
+        for (unsigned long long e = threadIdx.x; e < it.n; e += 256) a += in[e];
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) a += shfl_down_any(a, d);
+        if ((threadIdx.x & 31u) == 0) s_w[threadIdx.x >> 5] = a;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            T t = s_w[0];
+            for (int w = 1; w < 8; w++) t += s_w[w];
+            *reinterpret_cast<T*>(it.out) = t;
         }
     }
 }

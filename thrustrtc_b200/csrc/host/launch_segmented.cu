@@ -59,7 +59,7 @@ bool seg_run_cfg(void* keys, void* vals, void* scan, const unsigned long long* o
     }
     size_t grid = (size_t)per_sm * sms;
     if (grid > nseg) grid = nseg;
-    kernel<<<(unsigned)grid, 256, smem, s>>>((KB*)keys, (V*)vals, (V*)scan, tk, tv, off, queue, nseg, ctrl);
+    kernel<<<(unsigned)grid, 256, smem, s>>>((KB*)keys, (V*)vals, (V*)scan, tk, tv, off, queue, nseg, ctrl, nullptr);
     ktimer_mark("seg_sort_scan_kernel", s);
     count_launch(2);
     return TRTC_CUDA(cudaGetLastError());
