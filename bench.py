@@ -58,6 +58,9 @@ WORKLOADS = {
     # batched form: 100,000 lognormal segments (~2^26 pairs), each sorted then exclusive-scanned
     "segmented_c4": (100_000, "seg_sort_scan_kernel", 20, 20,
                      "Gkeys/s batched segmented sort+scan, 100k lognormal segments", "Gkeys/s"),
+    # serving form: a Poisson stream of mixed requests (bounded sample of the 200,000)
+    "serving_c5": (1000, None, None, None,
+                   "requests/s serving mix 60% sort_by_key 25% scan 15% reduce, sizes 2^10..2^24", "requests/s"),
 }
 
 M64 = (1 << 64) - 1
@@ -201,6 +204,28 @@ def cpu_run(workload, sample_n, threads):
         with cf.ThreadPoolExecutor(threads) as ex:
             pairs = sum(ex.map(one, idx))
         return time.perf_counter() - t0, threads, pairs
+    if workload == "serving_c5":
+        # the first sample_n requests of the mix, served one after another by the oracle
+        reqs = serving_requests(WORKLOADS["serving_c5"][0])[:sample_n]
+        rng = np.random.default_rng(0)
+        data = []
+        for kind, t, n in reqs:
+            if t == 8:
+                data.append(rng.standard_normal(n).astype(np.float32))
+            else:
+                data.append(rng.integers(0, 2**31, n).astype(np.uint32 if t == 5 else np.int64))
+        t0 = time.perf_counter()
+        for (kind, t, n), x in zip(reqs, data):
+            if kind == 0:
+                if x.dtype.itemsize == 4:
+                    O.sort_pairs32(x, np.arange(n, dtype=np.uint32), False, threads)
+                else:
+                    O.sort_by_key(x, np.arange(n, dtype=np.uint32))
+            elif kind == 1:
+                O.scan(x, exclusive=True, init=0)
+            else:
+                O.reduce(x)
+        return time.perf_counter() - t0, threads, sample_n
     x, v = gen_inputs(workload, sample_n)
     t0 = time.perf_counter()
     if workload == "sort_by_key_u32":
@@ -216,6 +241,8 @@ def units_per_s_to_metric(workload, units, seconds):
     """Throughput in the metric's unit: Gkeys/s for sorts, GB/s of algorithmic bytes otherwise."""
     if workload in ("sort_by_key_u32", "segmented_c4"):
         return units / seconds / 1e9
+    if workload == "serving_c5":
+        return units / seconds
     return units * WORKLOADS[workload][3] / seconds / 1e9
 
 
@@ -227,7 +254,7 @@ def run_reference(args):
     wl = args.workload
     n, _, _, _, metric, unit = WORKLOADS[wl]
     threads = cpu_threads()
-    sample = args.cpu_sample or {"sort_by_key_u32": 1 << 25, "segmented_c4": 20000}.get(wl, 1 << 27)
+    sample = args.cpu_sample or {"sort_by_key_u32": 1 << 25, "segmented_c4": 20000, "serving_c5": 16}.get(wl, 1 << 27)
     from oracle import oracle as O
     O.build()
     for _ in range(args.warmup):
@@ -237,7 +264,10 @@ def run_reference(args):
     threads = ts[0][1]
     units = sum(u for _, _, u in ts)
     value = units_per_s_to_metric(wl, units, tot)
-    if wl == "segmented_c4":
+    if wl == "serving_c5":
+        desc = ("the first %d requests of the mix per step, one after another, oracle restatement, sorts of "
+                "4-byte keys on %d host threads" % (sample, threads))
+    elif wl == "segmented_c4":
         desc = ("%d of the %d segments per step, spread over the batch; oracle sort + exclusive scan per "
                 "segment, %d host threads" % (sample, n, threads))
     else:
@@ -256,7 +286,8 @@ def run_reference(args):
 
 
 def _dtype(wl):
-    return {"sort_by_key_u32": "u32", "inclusive_scan_i32": "int32", "reduce_f32": "f32", "segmented_c4": "u32"}[wl]
+    return {"sort_by_key_u32": "u32", "inclusive_scan_i32": "int32", "reduce_f32": "f32", "segmented_c4": "u32",
+            "serving_c5": "u32/i64/f32"}[wl]
 
 
 def _config(wl, n, world):
@@ -265,6 +296,9 @@ def _config(wl, n, world):
     if wl == "sort_by_key_u32":
         base.update({"keys": "uint32 uniform over 32 bits", "values": "uint32 = index", "order": "ascending, stable",
                      "step": "restore the unsorted pairs from a pristine copy (untimed), then one sort (timed)"})
+    elif wl == "serving_c5":
+        base = {"workload": wl, "requests": n, "mix": "60% Sort_By_Key, 25% exclusive scan, 15% reduce",
+                "sizes": "log-uniform 2^10..2^24", "types": "uint32 / int64 / float", "parallelism": "1 GPU"}
     elif wl == "segmented_c4":
         base = {"workload": wl, "segments": n, "lengths": "lognormal median 256 sigma 1.5 clipped [1, 2^20]",
                 "keys": "uint32 uniform", "values": "uint32 = index", "parallelism": "replicas x%d" % world}
@@ -754,6 +788,169 @@ def run_segmented(args):
     return 0
 
 
+# ---------------------------------------------------------------- serving form
+def serving_requests(count, seed=0):
+    """(kind, type, n) per request: kinds 60/25/15 % (Sort_By_Key / exclusive scan / reduce),
+    element types uint32 / int64 / float in equal shares, sizes log-uniform on [2^10, 2^24]."""
+    h = splitmix64(seed, 2, 3 * count)
+    u = (h >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    kind = np.where(u[0::3] < 0.6, 0, np.where(u[0::3] < 0.85, 1, 2))
+    types = np.array([5, 6, 8])[np.minimum((u[1::3] * 3).astype(np.int64), 2)]
+    n = np.floor(2.0 ** (10 + 14 * u[2::3])).astype(np.int64)
+    return list(zip(kind.tolist(), types.tolist(), n.tolist()))
+
+
+def _srv_sigs(L):
+    L.trtc_server_create.restype = ctypes.c_void_p
+    L.trtc_server_create.argtypes = [ctypes.c_ulonglong, ctypes.c_int, ctypes.c_ulonglong]
+    L.trtc_server_submit.restype = ctypes.c_longlong
+    L.trtc_server_submit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 3 + \
+        [ctypes.c_ulonglong]
+    L.trtc_server_poll.restype = ctypes.c_int
+    L.trtc_server_poll.argtypes = [ctypes.c_void_p]
+    L.trtc_server_info.restype = ctypes.c_int
+    L.trtc_server_info.argtypes = [ctypes.c_void_p, ctypes.c_longlong] + [ctypes.POINTER(ctypes.c_double)] * 3
+    L.trtc_server_now.restype = ctypes.c_double
+    L.trtc_server_now.argtypes = [ctypes.c_void_p]
+    L.trtc_server_forget_done.argtypes = [ctypes.c_void_p]
+    L.trtc_server_destroy.argtypes = [ctypes.c_void_p]
+
+
+def run_serving(args):
+    """Poisson arrivals of mixed requests into the request server (continuous batching: 4
+    streams, coalescing of requests up to 2^16 elements, 32 GB admission budget) beside the
+    plain path (the same requests one call at a time, no coalescing, one stream).  Offered
+    load is swept over fractions of each path's closed-loop capacity."""
+    import torch
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: a CUDA device is required (there is no CPU path)")
+    if rank != 0:
+        return 0  # one GPU: the serving form is measured on rank 0 only
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import thrustrtc_b200 as trtc
+    from thrustrtc_b200 import _native as N
+    trtc.init()
+    L = N.lib
+    _srv_sigs(L)
+    count = args.n or WORKLOADS["serving_c5"][0]
+    reqs = serving_requests(count)
+    # device inputs: one pristine and one working slice per request, per element type
+    tot = {5: 0, 6: 0, 8: 0}
+    offs = []
+    for kind, t, n in reqs:
+        offs.append(tot[t])
+        tot[t] += n
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    pristine = {5: torch.randint(-2**31, 2**31 - 1, (max(tot[5], 1),), dtype=torch.int32, device=dev, generator=g),
+                6: torch.randint(-2**62, 2**62, (max(tot[6], 1),), dtype=torch.int64, device=dev, generator=g),
+                8: torch.randn(max(tot[8], 1), device=dev, generator=g)}
+    work = {t: torch.empty_like(x) for t, x in pristine.items()}
+    vals = torch.empty(sum(n for k, t, n in reqs if k == 0) + 1, dtype=torch.int32, device=dev)
+    outs = {t: torch.empty_like(x) for t, x in pristine.items()}
+    voff, acc = [], 0
+    for kind, t, n in reqs:
+        voff.append(acc)
+        acc += n if kind == 0 else 0
+    esz = {5: 4, 6: 8, 8: 4}
+
+    def ptrs(i):
+        kind, t, n = reqs[i]
+        k = ctypes.c_void_p(work[t].data_ptr() + esz[t] * offs[i])
+        v = ctypes.c_void_p(vals.data_ptr() + 4 * voff[i]) if kind == 0 else None
+        o = ctypes.c_void_p(outs[t].data_ptr() + esz[t] * offs[i]) if kind == 1 else None
+        return k, v, o
+
+    def restore():
+        for t in work:
+            work[t].copy_(pristine[t])
+        vals.copy_(torch.arange(vals.numel(), dtype=torch.int32, device=dev))
+        torch.cuda.synchronize()
+
+    def run_once(srv, arrivals):
+        """Submits request i at arrivals[i] (seconds from the start; None = all at once) and
+        polls until all are done; returns (latencies in s, makespan in s)."""
+        restore()
+        ids = [0] * count
+        t0 = L.trtc_server_now(srv)
+        nxt = 0
+        while True:
+            now = L.trtc_server_now(srv) - t0
+            while nxt < count and (arrivals is None or arrivals[nxt] <= now):
+                k, v, o = ptrs(nxt)
+                kind, t, n = reqs[nxt]
+                ids[nxt] = L.trtc_server_submit(srv, kind, t, k, v, o, n)
+                if ids[nxt] <= 0:
+                    raise RuntimeError(N.last_error())
+                nxt += 1
+            left = L.trtc_server_poll(srv)
+            if left < 0:
+                raise RuntimeError(N.last_error())
+            if nxt == count and left == 0:
+                break
+        lat, first, last = [], None, 0.0
+        ts, td = ctypes.c_double(), ctypes.c_double()
+        for rid in ids:
+            st = L.trtc_server_info(srv, rid, ctypes.byref(ts), ctypes.byref(td), None)
+            if st != 2:
+                raise RuntimeError("request %d not done (state %d)" % (rid, st))
+            lat.append(td.value - ts.value)
+            first = ts.value if first is None else min(first, ts.value)
+            last = max(last, td.value)
+        L.trtc_server_forget_done(srv)
+        return np.array(lat), last - first
+
+    def sweep(srv):
+        run_once(srv, None)  # warm-up (kernel set-up, memory pool)
+        _, span = run_once(srv, None)
+        cap = count / span
+        levels = []
+        for f in (0.10, 0.25, 0.50, 0.75, 0.90, 1.00, 1.10, 1.20):
+            rate = f * cap
+            h = splitmix64(1, 3, count)
+            u = ((h >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+            arrivals = np.cumsum(-np.log(u) / rate)
+            lat, span = run_once(srv, arrivals)
+            levels.append({"load": f, "offered_rps": rate, "achieved_rps": count / span,
+                           "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)})
+        return cap, levels
+
+    budget = 32 << 30
+    srv = L.trtc_server_create(budget, 4, 1 << 16)
+    if not srv:
+        raise RuntimeError(N.last_error())
+    lc0 = N.launch_count()
+    sampler = ClockSampler(dev)
+    with sampler:
+        cap_b, lv_b = sweep(srv)
+    launches = N.launch_count() - lc0
+    L.trtc_server_destroy(srv)
+    srv = L.trtc_server_create(budget, 1, 0)
+    cap_p, lv_p = sweep(srv)
+    L.trtc_server_destroy(srv)
+    elems = sum(n for _, _, n in reqs)
+    line = {"metric": WORKLOADS["serving_c5"][4], "value": cap_b, "unit": "requests/s", "n_gpus": 1,
+            "steps": len(lv_b), "warmup": 1, "ms_per_step": 1e3 * count / cap_b, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32/i64/f32",
+            "data": "synthetic (SplitMix64 seed 0 request mix; torch generator seed 0 contents)",
+            "config": {"workload": "serving_c5", "requests_per_level": count,
+                       "sample": "%d requests per load level (a bounded sample of the 200,000-request stream)" % count,
+                       "mix": "60% Sort_By_Key (+uint32 values), 25% exclusive scan, 15% reduce",
+                       "sizes": "log-uniform 2^10..2^24", "types": "uint32 / int64 / float equal shares",
+                       "elements_per_level": elems, "budget_bytes": budget,
+                       "server": "4 streams, coalescing up to 2^16 elements per request, admission by budget",
+                       "plain": "same requests, one call at a time on one stream, no coalescing",
+                       "load_levels": "fractions of each path's closed-loop capacity"},
+            "capacity_rps": {"served": cap_b, "plain": cap_p, "ratio": cap_b / cap_p},
+            "levels_served": lv_b, "levels_plain": lv_p,
+            "clocks": sampler.summary(), "gpu_launches": launches,
+            "e2e": None, "cpu_baseline": None, "roofline": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -777,6 +974,8 @@ def main():
         return run_reference(args)
     if args.workload == "segmented_c4":
         return run_segmented(args)
+    if args.workload == "serving_c5":
+        return run_serving(args)
     return run_ours(args)
 
 
