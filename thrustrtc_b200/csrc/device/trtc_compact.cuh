@@ -134,6 +134,159 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pre
     }
 }
 
+// Two-phase, persistent, software-pipelined form of compact_kernel for outputs that do not
+// overlap the inputs: phase 1 reads a tile, evaluates the selection and publishes its count;
+// phase 2 (after the look-back) reads the tile again -- normally from L2 -- and writes it.
+// A CTA runs phase 1 of its next tile before the look-back of its current one, so the waits
+// overlap HBM reads.  (In-place forms keep the one-pass kernel: a later tile may write into
+// an earlier tile's range before that tile re-reads it.)
+template <int MODE, bool PARTITION, bool TWO, class InV, class StV, class Pred, class ValT, class OutV, class FalseV,
+          class In2V, class Out2V, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pred pred, ValT value, OutV out,
+                                                         FalseV out_false, In2V in2, Out2V out2, size_t n,
+                                                         size_t tiles, LookbackState st) {
+    typedef typename remove_cvref<typename InV::value_t>::type E;
+    typedef typename remove_cvref<decltype(in2[0])>::type E2;
+    constexpr int WARPS = BLOCK / 32;
+    constexpr int TILE = BLOCK * ITEMS;
+    __shared__ unsigned long long s_ticket;
+    __shared__ uint32_t s_wcnt[2][WARPS];
+    __shared__ unsigned long long s_agg[2];
+    __shared__ unsigned long long s_pre;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint32_t ltm = lanemask_lt();
+
+    auto claim = [&]() -> size_t {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned long long t = atomicAdd(st.tile_ctr, 1ull);
+            if (t == (unsigned long long)tiles + gridDim.x - 1) atomicExch(st.tile_ctr, 0ull);
+            s_ticket = t;
+        }
+        __syncthreads();
+        return (size_t)s_ticket;
+    };
+    // loads the tile's elements of this thread and evaluates the selection
+    auto load = [&](size_t tile, E (&v)[ITEMS], bool (&f)[ITEMS]) {
+        const size_t wbase = tile * TILE + (size_t)warp * 32 * ITEMS;
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const size_t idx = wbase + (size_t)i * 32 + lane;
+            v[i] = idx < n ? (E)in[idx] : E();
+        }
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const size_t idx = wbase + (size_t)i * 32 + lane;
+            const bool ok = idx < n;
+            bool sel = false;
+            if constexpr (MODE == CM_PRED) sel = ok && (bool)pred(v[i]);
+            else if constexpr (MODE == CM_PRED_STENCIL) sel = ok && (bool)pred(stencil[idx < n ? idx : 0]);
+            else if constexpr (MODE == CM_NOT_EQUAL) sel = ok && !(v[i] == value);
+            else if constexpr (MODE == CM_NOT_PRED) sel = ok && !(bool)pred(v[i]);
+            else if constexpr (MODE == CM_NOT_PRED_STENCIL) sel = ok && !(bool)pred(stencil[idx < n ? idx : 0]);
+            else if constexpr (MODE == CM_UNIQUE || MODE == CM_UNIQUE_PRED) {
+                E prev = shfl_up_any(v[i], 1);
+                const E last = i > 0 ? shfl_any(v[i > 0 ? i - 1 : 0], 31) : E();
+                if (lane == 0) prev = (i > 0) ? last : ((ok && idx > 0) ? (E)in[idx - 1] : E());
+                if constexpr (MODE == CM_UNIQUE) sel = ok && (idx == 0 || v[i] != prev);
+                else sel = ok && (idx == 0 || !(bool)pred(v[i], prev));
+            } else if constexpr (MODE == CM_TAIL) {
+                E next = shfl_down_any(v[i], 1);
+                const E first = i + 1 < ITEMS ? shfl_any(v[i + 1 < ITEMS ? i + 1 : i], 0) : E();
+                if (lane == 31) next = (i + 1 < ITEMS) ? first : ((idx + 1 < n) ? (E)in[idx + 1] : E());
+                sel = ok && (idx + 1 == n || !(bool)pred(v[i], next));
+            }
+            f[i] = sel;
+        }
+    };
+    auto phase1 = [&](size_t tile, int b) {
+        E v[ITEMS];
+        bool f[ITEMS];
+        load(tile, v, f);
+        uint32_t wc = 0;
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) wc += (uint32_t)__popc(__ballot_sync(0xffffffffu, f[i]));
+        if (lane == 0) s_wcnt[b][warp] = wc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long agg = 0;
+            for (int w = 0; w < WARPS; w++) agg += s_wcnt[b][w];
+            s_agg[b] = agg;
+            if (tile == 0) {
+                publish<unsigned long long>(st, 0, agg, true, false);
+                if (tiles == 1 && st.result) *reinterpret_cast<unsigned long long*>(st.result) = agg;
+            } else {
+                publish<unsigned long long>(st, tile, agg, false, false);
+            }
+        }
+    };
+
+    size_t cur = claim();
+    if (cur >= tiles) return;
+    int buf = 0;
+    phase1(cur, 0);
+    while (true) {
+        const size_t nxt = claim();
+        if (nxt < tiles) phase1(nxt, buf ^ 1);
+        if (warp == 0) {
+            unsigned long long pre = 0;
+            if (cur > 0) {
+                Plus plus;
+                bool dummy;
+                pre = lookback_prefix<unsigned long long, Plus, false>(st, cur, plus, dummy).v;
+                if (lane == 0) {
+                    publish<unsigned long long>(st, cur, pre + s_agg[buf], true, false);
+                    if (cur == tiles - 1 && st.result) *reinterpret_cast<unsigned long long*>(st.result) = pre + s_agg[buf];
+                }
+            }
+            if (lane == 0) s_pre = pre;
+        }
+        __syncthreads();
+        {
+            E v[ITEMS];
+            bool f[ITEMS];
+            load(cur, v, f);
+            E2 v2[TWO ? ITEMS : 1];
+            const size_t wbase = cur * TILE + (size_t)warp * 32 * ITEMS;
+            if constexpr (TWO) {
+#pragma unroll
+                for (int i = 0; i < ITEMS; i++) {
+                    const size_t idx = wbase + (size_t)i * 32 + lane;
+                    v2[i] = idx < n ? (E2)in2[idx] : E2();
+                }
+            }
+            unsigned long long base = s_pre;
+            for (uint32_t w = 0; w < warp; w++) base += s_wcnt[buf][w];
+            const size_t out_n = out.size();
+            uint32_t wc = 0;
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t bal = __ballot_sync(0xffffffffu, f[i]);
+                const size_t idx = wbase + (size_t)i * 32 + lane;
+                const unsigned long long before = base + wc + (uint32_t)__popc(bal & ltm);
+                wc += (uint32_t)__popc(bal);
+                if (idx >= n) continue;
+                if (f[i]) {
+                    if (before < out_n) {
+                        out[before] = v[i];
+                        if constexpr (TWO) {
+                            if (before < (unsigned long long)out2.size()) out2[before] = v2[i];
+                        }
+                    }
+                } else {
+                    if constexpr (PARTITION) {
+                        const unsigned long long fp = idx - before;
+                        if (fp < (unsigned long long)out_false.size()) out_false[fp] = v[i];
+                    }
+                }
+            }
+        }
+        if (nxt >= tiles) break;
+        cur = nxt;
+        buf ^= 1;
+    }
+}
+
 // Partition in place: rejected elements were compacted into a temp buffer; move them
 // behind the selected ones once the count is known on the device.
 template <class E>

@@ -219,10 +219,27 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
     if (!fill_lookback(st, s, tiles, 8)) return false;
     VectorView<T> iv = make_view<T>(const_cast<T*>(in), n);
     VectorView<T> ov = make_view<T>(out, n);
+    const char* ib = (const char*)in;
+    const char* ob = (const char*)out;
+    const bool disjoint = ob + n * sizeof(T) <= ib || ib + n * sizeof(T) <= ob;
     ktimer_mark("", s);
-    compact_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing, Nothing, Nothing,
-                   SCAN_BLOCK, ITEMS><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(
-        iv, Nothing(), EqualTo(), value ? *value : T(), ov, Nothing(), Nothing(), Nothing(), n, st);
+    if (disjoint) {
+        // out-of-place: persistent two-phase tiles (the input is read twice, the second time
+        // normally from L2)
+        auto kernel = compact2_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing,
+                                      Nothing, Nothing, SCAN_BLOCK, ITEMS>;
+        static int per_sm = 0;
+        if (per_sm == 0 && !TRTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, SCAN_BLOCK, 0)))
+            return false;
+        size_t grid = (size_t)(per_sm > 0 ? per_sm : 1) * sm_count();
+        if (grid > tiles) grid = tiles;
+        kernel<<<(unsigned)grid, SCAN_BLOCK, 0, s>>>(iv, Nothing(), EqualTo(), value ? *value : T(), ov, Nothing(),
+                                                      Nothing(), Nothing(), n, tiles, st);
+    } else {
+        compact_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing, Nothing,
+                       Nothing, SCAN_BLOCK, ITEMS><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(
+            iv, Nothing(), EqualTo(), value ? *value : T(), ov, Nothing(), Nothing(), Nothing(), n, st);
+    }
     count_launch();
     ktimer_mark("compact_kernel", s);
     if (!TRTC_CUDA(cudaGetLastError())) return false;

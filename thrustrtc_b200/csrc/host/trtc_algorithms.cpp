@@ -464,6 +464,30 @@ struct CompactSpec {
     const DeviceViewable* value = nullptr;
     ViewArg out, out_false, in2, out2;
     bool partition = false, two = false;
+    std::vector<const DVVectorLike*> written, read;  // for the overlap test
+    void set_out(const DVVectorLike& v) { out = view_arg(v); written.push_back(&v); }
+    void set_false(const DVVectorLike& v) { out_false = view_arg(v); written.push_back(&v); }
+    void set_out2(const DVVectorLike& v) { out2 = view_arg(v); written.push_back(&v); }
+    void set_in2(const DVVectorLike& v) { in2 = view_arg(v); read.push_back(&v); }
+    // true when no written vector can share memory with a read one (both contiguous and
+    // their byte ranges disjoint)
+    bool disjoint() const {
+        std::vector<const DVVectorLike*> r(read);
+        r.push_back(in);
+        if (stencil) r.push_back(stencil);
+        for (const DVVectorLike* w : written) {
+            const char* wp = (const char*)w->contiguous_data();
+            if (!wp) return false;
+            const size_t wb = w->size() * w->elem_size();
+            for (const DVVectorLike* x : r) {
+                const char* xp = (const char*)x->contiguous_data();
+                if (!xp) return false;
+                const size_t xb = x->size() * x->elem_size();
+                if (!(wp + wb <= xp || xp + xb <= wp)) return false;
+            }
+        }
+        return true;
+    }
 };
 
 const unsigned long long kFail = ~0ull;
@@ -496,14 +520,22 @@ unsigned long long run_compact(CompactSpec& c) {
     ViewBuf st;
     trtc::LookbackState lst;
     if (!lookback_param(tiles, 8, st, &lst)) return kFail;
-    const std::string k = "trtc::compact_kernel<" + num(c.mode) + ", " + (c.partition ? "true" : "false") + ", " +
-                          (c.two ? "true" : "false") + ", " + iv.type + ", " + sv.type + ", " + ptype + ", " + vtype +
-                          ", " + c.out.type + ", " + c.out_false.type + ", " + c.in2.type + ", " + c.out2.type +
-                          ", 256, 16>";
-    if (!jit_run({"trtc_compact.cuh"}, k, (unsigned)tiles, 256,
-                 {iv.bytes, sv.bytes, pbytes, vbytes, c.out.bytes, c.out_false.bytes, c.in2.bytes, c.out2.bytes,
-                  pod_bytes<size_t>(n), st}))
-        return kFail;
+    const bool two_phase = c.disjoint();
+    const std::string k = std::string(two_phase ? "trtc::compact2_kernel<" : "trtc::compact_kernel<") + num(c.mode) +
+                          ", " + (c.partition ? "true" : "false") + ", " + (c.two ? "true" : "false") + ", " +
+                          iv.type + ", " + sv.type + ", " + ptype + ", " + vtype + ", " + c.out.type + ", " +
+                          c.out_false.type + ", " + c.in2.type + ", " + c.out2.type + ", 256, 16>";
+    std::vector<ViewBuf> params{iv.bytes, sv.bytes, pbytes, vbytes, c.out.bytes, c.out_false.bytes, c.in2.bytes,
+                                c.out2.bytes, pod_bytes<size_t>(n)};
+    unsigned grid = (unsigned)tiles;
+    if (two_phase) {
+        // persistent CTAs: 4 per SM (the kernel's register budget allows it for 4-byte elements)
+        const size_t g = (size_t)sm_count() * 4;
+        grid = (unsigned)(g < tiles ? g : tiles);
+        params.push_back(pod_bytes<size_t>(tiles));
+    }
+    params.push_back(st);
+    if (!jit_run({"trtc_compact.cuh"}, k, grid, 256, params)) return kFail;
     unsigned long long cnt = 0;
     if (!TRTC_CUDA(cudaMemcpyAsync(&cnt, lst.result, 8, cudaMemcpyDeviceToHost, S())) ||
         !check_device_errors(S(), "compaction"))
@@ -530,20 +562,20 @@ bool fast_compact(int mode, const DVVectorLike& in, DVVectorLike& out, const Dev
 
 uint32_t TRTC_Copy_If(const DVVectorLike& vec_in, DVVectorLike& vec_out, const Functor& pred) {
     CompactSpec c;
-    c.mode = CM_PRED; c.in = &vec_in; c.pred = &pred; c.out = view_arg(vec_out);
+    c.mode = CM_PRED; c.in = &vec_in; c.pred = &pred; c.set_out(vec_out);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Copy_If_Stencil(const DVVectorLike& vec_in, const DVVectorLike& vec_stencil, DVVectorLike& vec_out,
                               const Functor& pred) {
     CompactSpec c;
-    c.mode = CM_PRED_STENCIL; c.in = &vec_in; c.stencil = &vec_stencil; c.pred = &pred; c.out = view_arg(vec_out);
+    c.mode = CM_PRED_STENCIL; c.in = &vec_in; c.stencil = &vec_stencil; c.pred = &pred; c.set_out(vec_out);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Remove_Copy(const DVVectorLike& vec_in, DVVectorLike& vec_out, const DeviceViewable& value) {
     unsigned long long cnt = 0;
     if (fast_compact(CM_NOT_EQUAL, vec_in, vec_out, &value, cnt)) return to_u32(cnt);
     CompactSpec c;
-    c.mode = CM_NOT_EQUAL; c.in = &vec_in; c.value = &value; c.out = view_arg(vec_out);
+    c.mode = CM_NOT_EQUAL; c.in = &vec_in; c.value = &value; c.set_out(vec_out);
     return to_u32(run_compact(c));
 }
 // in place: a tile reads its input before anything is published, and selected elements only
@@ -551,14 +583,14 @@ uint32_t TRTC_Remove_Copy(const DVVectorLike& vec_in, DVVectorLike& vec_out, con
 uint32_t TRTC_Remove(DVVectorLike& vec, const DeviceViewable& value) { return TRTC_Remove_Copy(vec, vec, value); }
 uint32_t TRTC_Remove_Copy_If(const DVVectorLike& vec_in, DVVectorLike& vec_out, const Functor& pred) {
     CompactSpec c;
-    c.mode = CM_NOT_PRED; c.in = &vec_in; c.pred = &pred; c.out = view_arg(vec_out);
+    c.mode = CM_NOT_PRED; c.in = &vec_in; c.pred = &pred; c.set_out(vec_out);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Remove_If(DVVectorLike& vec, const Functor& pred) { return TRTC_Remove_Copy_If(vec, vec, pred); }
 uint32_t TRTC_Remove_Copy_If_Stencil(const DVVectorLike& vec_in, const DVVectorLike& stencil, DVVectorLike& vec_out,
                                      const Functor& pred) {
     CompactSpec c;
-    c.mode = CM_NOT_PRED_STENCIL; c.in = &vec_in; c.stencil = &stencil; c.pred = &pred; c.out = view_arg(vec_out);
+    c.mode = CM_NOT_PRED_STENCIL; c.in = &vec_in; c.stencil = &stencil; c.pred = &pred; c.set_out(vec_out);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Remove_If_Stencil(DVVectorLike& vec, const DVVectorLike& stencil, const Functor& pred) {
@@ -568,13 +600,13 @@ uint32_t TRTC_Unique_Copy(const DVVectorLike& vec_in, DVVectorLike& vec_out) {
     unsigned long long cnt = 0;
     if (fast_compact(CM_UNIQUE, vec_in, vec_out, nullptr, cnt)) return to_u32(cnt);
     CompactSpec c;
-    c.mode = CM_UNIQUE; c.in = &vec_in; c.out = view_arg(vec_out);
+    c.mode = CM_UNIQUE; c.in = &vec_in; c.set_out(vec_out);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Unique_Copy(const DVVectorLike& vec_in, DVVectorLike& vec_out, const Functor& binary_pred) {
     if (is_builtin(binary_pred, "EqualTo")) return TRTC_Unique_Copy(vec_in, vec_out);
     CompactSpec c;
-    c.mode = CM_UNIQUE_PRED; c.in = &vec_in; c.pred = &binary_pred; c.out = view_arg(vec_out);
+    c.mode = CM_UNIQUE_PRED; c.in = &vec_in; c.pred = &binary_pred; c.set_out(vec_out);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Unique(DVVectorLike& vec) { return TRTC_Unique_Copy(vec, vec); }
@@ -583,8 +615,8 @@ uint32_t TRTC_Unique_By_Key_Copy(const DVVectorLike& keys_in, const DVVectorLike
                                  DVVectorLike& values_out, const Functor& binary_pred) {
     CompactSpec c;
     c.mode = is_builtin(binary_pred, "EqualTo") ? CM_UNIQUE : CM_UNIQUE_PRED;
-    c.in = &keys_in; c.pred = &binary_pred; c.out = view_arg(keys_out);
-    c.two = true; c.in2 = view_arg(values_in); c.out2 = view_arg(values_out);
+    c.in = &keys_in; c.pred = &binary_pred; c.set_out(keys_out);
+    c.two = true; c.set_in2(values_in); c.set_out2(values_out);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Unique_By_Key_Copy(const DVVectorLike& keys_in, const DVVectorLike& values_in, DVVectorLike& keys_out,
@@ -603,14 +635,14 @@ uint32_t TRTC_Partition_Copy(const DVVectorLike& vec_in, DVVectorLike& vec_true,
                              const Functor& pred) {
     CompactSpec c;
     c.mode = CM_PRED; c.in = &vec_in; c.pred = &pred; c.partition = true;
-    c.out = view_arg(vec_true); c.out_false = view_arg(vec_false);
+    c.set_out(vec_true); c.set_false(vec_false);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Partition_Copy_Stencil(const DVVectorLike& vec_in, const DVVectorLike& stencil, DVVectorLike& vec_true,
                                      DVVectorLike& vec_false, const Functor& pred) {
     CompactSpec c;
     c.mode = CM_PRED_STENCIL; c.in = &vec_in; c.stencil = &stencil; c.pred = &pred; c.partition = true;
-    c.out = view_arg(vec_true); c.out_false = view_arg(vec_false);
+    c.set_out(vec_true); c.set_false(vec_false);
     return to_u32(run_compact(c));
 }
 // in place: selected elements are compacted in place, rejected ones into a temporary that is
@@ -624,7 +656,7 @@ static uint32_t partition_in_place(DVVectorLike& vec, const DVVectorLike* stenci
     const ViewArg tv = raw_view(tmp, n, vec.name_elem_cls());
     CompactSpec c;
     c.mode = stencil ? CM_PRED_STENCIL : CM_PRED; c.in = &vec; c.stencil = stencil; c.pred = &pred;
-    c.partition = true; c.out = view_arg(vec); c.out_false = tv;
+    c.partition = true; c.set_out(vec); c.out_false = tv;
     const unsigned long long cnt = run_compact(c);
     bool ok = cnt != kFail;
     if (ok && cnt < n) {
@@ -648,8 +680,8 @@ static uint32_t reduce_by_key_impl(const DVVectorLike& key_in, const DVVectorLik
     DVVector scanned(value_out.name_elem_cls().c_str(), n);
     if (!scan_by_key_dispatch(key_in, value_in, scanned, pred, op, false, nullptr)) return (uint32_t)(-1);
     CompactSpec c;
-    c.mode = CM_TAIL; c.in = &key_in; c.pred = &pred; c.out = view_arg(key_out);
-    c.two = true; c.in2 = view_arg(scanned); c.out2 = view_arg(value_out);
+    c.mode = CM_TAIL; c.in = &key_in; c.pred = &pred; c.set_out(key_out);
+    c.two = true; c.set_in2(scanned); c.set_out2(value_out);
     return to_u32(run_compact(c));
 }
 uint32_t TRTC_Reduce_By_Key(const DVVectorLike& key_in, const DVVectorLike& value_in, DVVectorLike& key_out,
