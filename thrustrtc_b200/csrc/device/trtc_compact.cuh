@@ -24,8 +24,10 @@ enum CompactMode : int {
     CM_TAIL = 7,             // i == n-1 || !pred(in[i], in[i+1]) reduce_by_key segment tails
 };
 
+// CT: type of the selected counts (32-bit while n < 2^32: flag and count then travel in one
+// 64-bit look-back word)
 template <int MODE, bool PARTITION, bool TWO, class InV, class StV, class Pred, class ValT, class OutV, class FalseV,
-          class In2V, class Out2V, int BLOCK, int ITEMS>
+          class In2V, class Out2V, int BLOCK, int ITEMS, class CT = unsigned long long>
 __global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pred pred, ValT value, OutV out,
                                                         FalseV out_false, In2V in2, Out2V out2, size_t n,
                                                         LookbackState st) {
@@ -35,7 +37,7 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pre
     constexpr int TILE = BLOCK * ITEMS;
     __shared__ uint32_t s_slot[2];
     __shared__ uint32_t s_wcnt[WARPS];
-    __shared__ unsigned long long s_pre;
+    __shared__ CT s_pre;
 
     const size_t tile = claim_tile(st, s_slot);
     const size_t tile_base = tile * TILE;
@@ -90,21 +92,21 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pre
     __syncthreads();
 
     if (warp == 0) {
-        unsigned long long agg = 0;
+        CT agg = 0;
         if (lane < (uint32_t)WARPS) agg = s_wcnt[lane];
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) agg += __shfl_down_sync(0xffffffffu, agg, d);
         agg = __shfl_sync(0xffffffffu, agg, 0);
-        unsigned long long pre = 0;
+        CT pre = 0;
         Plus plus;
         if (tile > 0) {
-            if (lane == 0) publish<unsigned long long>(st, tile, agg, false, false);
+            if (lane == 0) publish<CT>(st, tile, agg, false, false);
             bool dummy;
-            pre = lookback_prefix<unsigned long long, Plus, false>(st, tile, plus, dummy).v;
+            pre = lookback_prefix<CT, Plus, false>(st, tile, plus, dummy).v;
         }
         if (lane == 0) {
-            publish<unsigned long long>(st, tile, pre + agg, true, false);
-            if (tile_base + TILE >= n && st.result) *reinterpret_cast<unsigned long long*>(st.result) = pre + agg;
+            publish<CT>(st, tile, pre + agg, true, false);
+            if (tile_base + TILE >= n && st.result) *reinterpret_cast<unsigned long long*>(st.result) = (unsigned long long)(pre + agg);
             s_pre = pre;
         }
     }
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pre
 // overlap HBM reads.  (In-place forms keep the one-pass kernel: a later tile may write into
 // an earlier tile's range before that tile re-reads it.)
 template <int MODE, bool PARTITION, bool TWO, class InV, class StV, class Pred, class ValT, class OutV, class FalseV,
-          class In2V, class Out2V, int BLOCK, int ITEMS>
+          class In2V, class Out2V, int BLOCK, int ITEMS, class CT = unsigned long long>
 __global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pred pred, ValT value, OutV out,
                                                          FalseV out_false, In2V in2, Out2V out2, size_t n,
                                                          size_t tiles, LookbackState st) {
@@ -151,8 +153,8 @@ __global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pr
     constexpr int TILE = BLOCK * ITEMS;
     __shared__ unsigned long long s_ticket;
     __shared__ uint32_t s_wcnt[2][WARPS];
-    __shared__ unsigned long long s_agg[2];
-    __shared__ unsigned long long s_pre;
+    __shared__ CT s_agg[2];
+    __shared__ CT s_pre;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     const uint32_t ltm = lanemask_lt();
 
@@ -209,14 +211,14 @@ __global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pr
         if (lane == 0) s_wcnt[b][warp] = wc;
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned long long agg = 0;
+            CT agg = 0;
             for (int w = 0; w < WARPS; w++) agg += s_wcnt[b][w];
             s_agg[b] = agg;
             if (tile == 0) {
-                publish<unsigned long long>(st, 0, agg, true, false);
-                if (tiles == 1 && st.result) *reinterpret_cast<unsigned long long*>(st.result) = agg;
+                publish<CT>(st, 0, agg, true, false);
+                if (tiles == 1 && st.result) *reinterpret_cast<unsigned long long*>(st.result) = (unsigned long long)agg;
             } else {
-                publish<unsigned long long>(st, tile, agg, false, false);
+                publish<CT>(st, tile, agg, false, false);
             }
         }
     };
@@ -229,14 +231,14 @@ __global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pr
         const size_t nxt = claim();
         if (nxt < tiles) phase1(nxt, buf ^ 1);
         if (warp == 0) {
-            unsigned long long pre = 0;
+            CT pre = 0;
             if (cur > 0) {
                 Plus plus;
                 bool dummy;
-                pre = lookback_prefix<unsigned long long, Plus, false>(st, cur, plus, dummy).v;
+                pre = lookback_prefix<CT, Plus, false>(st, cur, plus, dummy).v;
                 if (lane == 0) {
-                    publish<unsigned long long>(st, cur, pre + s_agg[buf], true, false);
-                    if (cur == tiles - 1 && st.result) *reinterpret_cast<unsigned long long*>(st.result) = pre + s_agg[buf];
+                    publish<CT>(st, cur, (CT)(pre + s_agg[buf]), true, false);
+                    if (cur == tiles - 1 && st.result) *reinterpret_cast<unsigned long long*>(st.result) = (unsigned long long)(pre + s_agg[buf]);
                 }
             }
             if (lane == 0) s_pre = pre;

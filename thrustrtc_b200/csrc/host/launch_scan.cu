@@ -210,7 +210,7 @@ bool scan_by_key_raw(int ktc, int vtc, int mode, const void* keys, const void* v
 }
 
 // ---------------------------------------------------------------- compaction (built-in selectors)
-template <class T, int MODE>
+template <class T, int MODE, class CT>
 static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_t s, unsigned long long* count) {
     constexpr int ITEMS = 16;
     constexpr int TILE = SCAN_BLOCK * ITEMS;
@@ -227,7 +227,7 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
         // out-of-place: persistent two-phase tiles (the input is read twice, the second time
         // normally from L2)
         auto kernel = compact2_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing,
-                                      Nothing, Nothing, SCAN_BLOCK, ITEMS>;
+                                      Nothing, Nothing, SCAN_BLOCK, ITEMS, CT>;
         static int per_sm = 0;
         if (per_sm == 0 && !TRTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, SCAN_BLOCK, 0)))
             return false;
@@ -237,7 +237,7 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
                                                       Nothing(), Nothing(), n, tiles, st);
     } else {
         compact_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing, Nothing,
-                       Nothing, SCAN_BLOCK, ITEMS><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(
+                       Nothing, SCAN_BLOCK, ITEMS, CT><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(
             iv, Nothing(), EqualTo(), value ? *value : T(), ov, Nothing(), Nothing(), Nothing(), n, st);
     }
     count_launch();
@@ -250,8 +250,14 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
 template <class T>
 static bool compact_m(int mode, const void* in, void* out, size_t n, const void* value, cudaStream_t s,
                       unsigned long long* count) {
-    if (mode == CM_NOT_EQUAL) return compact_t<T, CM_NOT_EQUAL>((const T*)in, (T*)out, n, (const T*)value, s, count);
-    if (mode == CM_UNIQUE) return compact_t<T, CM_UNIQUE>((const T*)in, (T*)out, n, nullptr, s, count);
+    // 32-bit counts below 2^32 elements (packed look-back words)
+    const bool c32 = n < (1ull << 32);
+    if (mode == CM_NOT_EQUAL)
+        return c32 ? compact_t<T, CM_NOT_EQUAL, uint32_t>((const T*)in, (T*)out, n, (const T*)value, s, count)
+                   : compact_t<T, CM_NOT_EQUAL, unsigned long long>((const T*)in, (T*)out, n, (const T*)value, s, count);
+    if (mode == CM_UNIQUE)
+        return c32 ? compact_t<T, CM_UNIQUE, uint32_t>((const T*)in, (T*)out, n, nullptr, s, count)
+                   : compact_t<T, CM_UNIQUE, unsigned long long>((const T*)in, (T*)out, n, nullptr, s, count);
     set_error("compaction: unsupported built-in mode");
     return false;
 }

@@ -519,12 +519,14 @@ unsigned long long run_compact(CompactSpec& c) {
     const size_t tiles = (n + tile - 1) / tile;
     ViewBuf st;
     trtc::LookbackState lst;
-    if (!lookback_param(tiles, 8, st, &lst)) return kFail;
+    const bool c32 = n < (1ull << 32);  // 32-bit counts: flag and count in one look-back word
+    if (!lookback_param(tiles, c32 ? 4 : 8, st, &lst)) return kFail;
     const bool two_phase = c.disjoint();
     const std::string k = std::string(two_phase ? "trtc::compact2_kernel<" : "trtc::compact_kernel<") + num(c.mode) +
                           ", " + (c.partition ? "true" : "false") + ", " + (c.two ? "true" : "false") + ", " +
                           iv.type + ", " + sv.type + ", " + ptype + ", " + vtype + ", " + c.out.type + ", " +
-                          c.out_false.type + ", " + c.in2.type + ", " + c.out2.type + ", 256, 16>";
+                          c.out_false.type + ", " + c.in2.type + ", " + c.out2.type + ", 256, 16, " +
+                          (c32 ? "unsigned int" : "unsigned long long") + ">";
     std::vector<ViewBuf> params{iv.bytes, sv.bytes, pbytes, vbytes, c.out.bytes, c.out_false.bytes, c.in2.bytes,
                                 c.out2.bytes, pod_bytes<size_t>(n)};
     unsigned grid = (unsigned)tiles;
