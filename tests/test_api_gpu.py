@@ -286,3 +286,28 @@ def test_for_and_kernel(trtc):
                                    "    if (i < n) vec[i] = vec[i] + 1;\n")
     k.launch(4, 256, [v, trtc.DVUInt32(1000)])
     assert v.to_host().tolist() == [3 * i + 1 for i in range(1000)]
+
+
+def test_compaction_alignment_and_extremes(trtc):
+    # aligned full tiles (16-byte vector path), misaligned sub-ranges (element path), all / none kept
+    rng = np.random.default_rng(12)
+    n = 3 * 4096 + 1000
+    x = rng.integers(-2**31, 2**31 - 1, n, dtype=np.int64).astype(np.int32)
+    d = trtc.device_vector_from_numpy(x)
+    odd = trtc.Functor({}, ["x"], "        return (x & 1) != 0;\n")
+    for off in (0, 1, 3, 4):
+        src = trtc.DVRange(d, off, n)
+        o = trtc.device_vector("int32_t", n)
+        c = trtc.Copy_If(src, o, odd)
+        xs = x[off:]
+        exp = xs[(xs & 1) != 0]
+        assert c == len(exp) and o.to_host(0, c).tolist() == exp.tolist(), off
+    allk = trtc.Functor({}, ["x"], "        return true;\n")
+    nonek = trtc.Functor({}, ["x"], "        return false;\n")
+    o = trtc.device_vector("int32_t", n)
+    assert trtc.Copy_If(d, o, allk) == n and o.to_host().tolist() == x.tolist()
+    assert trtc.Copy_If(d, o, nonek) == 0
+    r = trtc.device_vector("int32_t", n)
+    c = trtc.Remove_Copy(d, r, trtc.DVInt32(int(x[5])))
+    exp = x[x != x[5]]
+    assert c == len(exp) and r.to_host(0, c).tolist() == exp.tolist()

@@ -137,14 +137,14 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pre
 }
 
 // Two-phase, persistent, software-pipelined form of compact_kernel for outputs that do not
-// overlap the inputs: phase 1 reads a tile, evaluates the selection and publishes its count;
+// overlap the inputs (compiled for 4 resident CTAs per SM, the persistent grid's size): phase 1 reads a tile, evaluates the selection and publishes its count;
 // phase 2 (after the look-back) reads the tile again -- normally from L2 -- and writes it.
 // A CTA runs phase 1 of its next tile before the look-back of its current one, so the waits
 // overlap HBM reads.  (In-place forms keep the one-pass kernel: a later tile may write into
 // an earlier tile's range before that tile re-reads it.)
 template <int MODE, bool PARTITION, bool TWO, class InV, class StV, class Pred, class ValT, class OutV, class FalseV,
           class In2V, class Out2V, int BLOCK, int ITEMS, class CT = unsigned long long>
-__global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pred pred, ValT value, OutV out,
+__global__ void __launch_bounds__(BLOCK, 4) compact2_kernel(InV in, StV stencil, Pred pred, ValT value, OutV out,
                                                          FalseV out_false, In2V in2, Out2V out2, size_t n,
                                                          size_t tiles, LookbackState st) {
     typedef typename remove_cvref<typename InV::value_t>::type E;
@@ -157,6 +157,21 @@ __global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pr
     __shared__ CT s_pre;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     const uint32_t ltm = lanemask_lt();
+    // 16-byte vector path for full, aligned tiles of 4-byte elements under element-wise
+    // selections: lane l of a warp row holds 4 consecutive elements
+    constexpr bool VECOK = ViewTraits<InV>::contiguous && ViewTraits<OutV>::contiguous && sizeof(E) == 4 && !TWO &&
+                           !PARTITION && (MODE == CM_PRED || MODE == CM_NOT_EQUAL || MODE == CM_NOT_PRED);
+    constexpr int VROWS = ITEMS / 4;
+    typedef union { uint4 q; E t[4]; } Vec;
+    auto vec_fast = [&](size_t tile) -> bool {
+        if constexpr (VECOK) return (tile + 1) * (size_t)TILE <= n && ((((size_t)in._data) & 15) == 0);
+        else return false;
+    };
+    auto vsel = [&](const E& x) -> bool {
+        if constexpr (MODE == CM_PRED) return (bool)pred(x);
+        else if constexpr (MODE == CM_NOT_EQUAL) return !(x == value);
+        else return !(bool)pred(x);
+    };
 
     auto claim = [&]() -> size_t {
         __syncthreads();
@@ -202,12 +217,27 @@ __global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pr
         }
     };
     auto phase1 = [&](size_t tile, int b) {
-        E v[ITEMS];
-        bool f[ITEMS];
-        load(tile, v, f);
         uint32_t wc = 0;
+        if (vec_fast(tile)) {
+            if constexpr (VECOK) {
+                const uint4* p = reinterpret_cast<const uint4*>(in._data + tile * TILE + (size_t)warp * 32 * ITEMS);
+                uint32_t c = 0;
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++) wc += (uint32_t)__popc(__ballot_sync(0xffffffffu, f[i]));
+                for (int r = 0; r < VROWS; r++) {
+                    Vec u;
+                    u.q = p[r * 32 + lane];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) c += vsel(u.t[e]) ? 1u : 0u;
+                }
+                wc = __reduce_add_sync(0xffffffffu, c);
+            }
+        } else {
+            E v[ITEMS];
+            bool f[ITEMS];
+            load(tile, v, f);
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) wc += (uint32_t)__popc(__ballot_sync(0xffffffffu, f[i]));
+        }
         if (lane == 0) s_wcnt[b][warp] = wc;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -244,7 +274,39 @@ __global__ void __launch_bounds__(BLOCK) compact2_kernel(InV in, StV stencil, Pr
             if (lane == 0) s_pre = pre;
         }
         __syncthreads();
-        {
+        if (vec_fast(cur)) {
+            if constexpr (VECOK) {
+                unsigned long long run = s_pre;
+                for (uint32_t w = 0; w < warp; w++) run += s_wcnt[buf][w];
+                const uint4* p = reinterpret_cast<const uint4*>(in._data + cur * TILE + (size_t)warp * 32 * ITEMS);
+                Vec u[VROWS];
+#pragma unroll
+                for (int r = 0; r < VROWS; r++) u[r].q = p[r * 32 + lane];
+                const unsigned long long out_n = out.size();
+#pragma unroll
+                for (int r = 0; r < VROWS; r++) {
+                    bool f[4];
+                    uint32_t c = 0;
+#pragma unroll
+                    for (int e = 0; e < 4; e++) { f[e] = vsel(u[r].t[e]); c += f[e] ? 1u : 0u; }
+                    uint32_t x = c;  // inclusive prefix of the lane counts
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+                        if (lane >= (uint32_t)d) x += y;
+                    }
+                    unsigned long long pos = run + (x - c);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        if (f[e]) {
+                            if (pos < out_n) out._data[pos] = u[r].t[e];
+                            pos++;
+                        }
+                    }
+                    run += __shfl_sync(0xffffffffu, x, 31);
+                }
+            }
+        } else {
             E v[ITEMS];
             bool f[ITEMS];
             load(cur, v, f);

@@ -210,24 +210,29 @@ bool scan_by_key_raw(int ktc, int vtc, int mode, const void* keys, const void* v
 }
 
 // ---------------------------------------------------------------- compaction (built-in selectors)
+#ifndef TRTC_COMPACT2_ITEMS
+#define TRTC_COMPACT2_ITEMS 32  // elements per thread of a two-phase compaction tile
+#endif
+
 template <class T, int MODE, class CT>
 static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_t s, unsigned long long* count) {
-    constexpr int ITEMS = 16;
-    constexpr int TILE = SCAN_BLOCK * ITEMS;
+    const char* ib = (const char*)in;
+    const char* ob = (const char*)out;
+    const bool disjoint = ob + n * sizeof(T) <= ib || ib + n * sizeof(T) <= ob;
+    constexpr int ITEMS1 = 16, ITEMS2 = TRTC_COMPACT2_ITEMS;
+    const int ITEMS = disjoint ? ITEMS2 : ITEMS1;
+    const size_t TILE = (size_t)SCAN_BLOCK * ITEMS;
     const size_t tiles = (n + TILE - 1) / TILE;
     LookbackState st;
     if (!fill_lookback(st, s, tiles, 8)) return false;
     VectorView<T> iv = make_view<T>(const_cast<T*>(in), n);
     VectorView<T> ov = make_view<T>(out, n);
-    const char* ib = (const char*)in;
-    const char* ob = (const char*)out;
-    const bool disjoint = ob + n * sizeof(T) <= ib || ib + n * sizeof(T) <= ob;
     ktimer_mark("", s);
     if (disjoint) {
         // out-of-place: persistent two-phase tiles (the input is read twice, the second time
         // normally from L2)
         auto kernel = compact2_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing,
-                                      Nothing, Nothing, SCAN_BLOCK, ITEMS, CT>;
+                                      Nothing, Nothing, SCAN_BLOCK, ITEMS2, CT>;
         static int per_sm = 0;
         if (per_sm == 0 && !TRTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, SCAN_BLOCK, 0)))
             return false;
@@ -237,7 +242,7 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
                                                       Nothing(), Nothing(), n, tiles, st);
     } else {
         compact_kernel<MODE, false, false, VectorView<T>, Nothing, EqualTo, T, VectorView<T>, Nothing, Nothing,
-                       Nothing, SCAN_BLOCK, ITEMS, CT><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(
+                       Nothing, SCAN_BLOCK, ITEMS1, CT><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(
             iv, Nothing(), EqualTo(), value ? *value : T(), ov, Nothing(), Nothing(), Nothing(), n, st);
     }
     count_launch();

@@ -515,17 +515,18 @@ unsigned long long run_compact(CompactSpec& c) {
     }
     const std::string ptype = c.pred ? c.pred->name_view_cls() : "EqualTo";
     const ViewBuf pbytes = c.pred ? c.pred->view() : nothing_bytes();
-    const size_t tile = 256 * 16;
+    const bool two_phase = c.disjoint();
+    const size_t tile = 256 * (two_phase ? 32 : 16);
     const size_t tiles = (n + tile - 1) / tile;
     ViewBuf st;
     trtc::LookbackState lst;
     const bool c32 = n < (1ull << 32);  // 32-bit counts: flag and count in one look-back word
     if (!lookback_param(tiles, c32 ? 4 : 8, st, &lst)) return kFail;
-    const bool two_phase = c.disjoint();
     const std::string k = std::string(two_phase ? "trtc::compact2_kernel<" : "trtc::compact_kernel<") + num(c.mode) +
                           ", " + (c.partition ? "true" : "false") + ", " + (c.two ? "true" : "false") + ", " +
                           iv.type + ", " + sv.type + ", " + ptype + ", " + vtype + ", " + c.out.type + ", " +
-                          c.out_false.type + ", " + c.in2.type + ", " + c.out2.type + ", 256, 16, " +
+                          c.out_false.type + ", " + c.in2.type + ", " + c.out2.type + ", 256, " +
+                          (two_phase ? "32, " : "16, ") +
                           (c32 ? "unsigned int" : "unsigned long long") + ">";
     std::vector<ViewBuf> params{iv.bytes, sv.bytes, pbytes, vbytes, c.out.bytes, c.out_false.bytes, c.in2.bytes,
                                 c.out2.bytes, pod_bytes<size_t>(n)};
