@@ -116,6 +116,14 @@ unsigned n_reduce_by_key(void* ptr_key_in, void* ptr_value_in, void* ptr_key_out
 unsigned long long n_min_element(void* ptr_vec, void* ptr_comp);
 void* n_transform_reduce(void* ptr_vec, void* ptr_unary_op, void* ptr_init, void* ptr_binary_op);
 
+/* searches in a sorted vector -- python/api.h:175-180 */
+unsigned long long n_lower_bound(void* ptr_vec, void* ptr_value, void* ptr_comp);
+unsigned long long n_upper_bound(void* ptr_vec, void* ptr_value, void* ptr_comp);
+int n_binary_search(void* ptr_vec, void* ptr_value, void* ptr_comp);
+int n_lower_bound_v(void* ptr_vec, void* ptr_values, void* ptr_result, void* ptr_comp);
+int n_upper_bound_v(void* ptr_vec, void* ptr_values, void* ptr_result, void* ptr_comp);
+int n_binary_search_v(void* ptr_vec, void* ptr_values, void* ptr_result, void* ptr_comp);
+
 /* prefix sums -- python/api.h:144-150 */
 int n_inclusive_scan(void* ptr_vec_in, void* ptr_vec_out, void* ptr_binary_op);
 int n_exclusive_scan(void* ptr_vec_in, void* ptr_vec_out, void* ptr_init, void* ptr_binary_op);

@@ -361,6 +361,26 @@ THRUST_RTC_API bool TRTC_Transform_Reduce(const DVVectorLike& vec, const Functor
                                           const Functor& binary_op, ViewBuf& ret);
 THRUST_RTC_API bool TRTC_Min_Element(const DVVectorLike& vec, size_t& id_min);
 
+// searches in a sorted view -- binary_search.h:10-25
+THRUST_RTC_API bool TRTC_Lower_Bound(const DVVectorLike& vec, const DeviceViewable& value, size_t& result);
+THRUST_RTC_API bool TRTC_Lower_Bound(const DVVectorLike& vec, const DeviceViewable& value, const Functor& comp,
+                                     size_t& result);
+THRUST_RTC_API bool TRTC_Upper_Bound(const DVVectorLike& vec, const DeviceViewable& value, size_t& result);
+THRUST_RTC_API bool TRTC_Upper_Bound(const DVVectorLike& vec, const DeviceViewable& value, const Functor& comp,
+                                     size_t& result);
+THRUST_RTC_API bool TRTC_Binary_Search(const DVVectorLike& vec, const DeviceViewable& value, bool& result);
+THRUST_RTC_API bool TRTC_Binary_Search(const DVVectorLike& vec, const DeviceViewable& value, const Functor& comp,
+                                       bool& result);
+THRUST_RTC_API bool TRTC_Lower_Bound_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result);
+THRUST_RTC_API bool TRTC_Lower_Bound_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result,
+                                       const Functor& comp);
+THRUST_RTC_API bool TRTC_Upper_Bound_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result);
+THRUST_RTC_API bool TRTC_Upper_Bound_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result,
+                                       const Functor& comp);
+THRUST_RTC_API bool TRTC_Binary_Search_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result);
+THRUST_RTC_API bool TRTC_Binary_Search_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result,
+                                         const Functor& comp);
+
 THRUST_RTC_API bool TRTC_Copy(const DVVectorLike& vec_in, DVVectorLike& vec_out);
 THRUST_RTC_API uint32_t TRTC_Copy_If(const DVVectorLike& vec_in, DVVectorLike& vec_out, const Functor& pred);
 THRUST_RTC_API uint32_t TRTC_Copy_If_Stencil(const DVVectorLike& vec_in, const DVVectorLike& vec_stencil,

@@ -311,3 +311,43 @@ def test_compaction_alignment_and_extremes(trtc):
     c = trtc.Remove_Copy(d, r, trtc.DVInt32(int(x[5])))
     exp = x[x != x[5]]
     assert c == len(exp) and r.to_host(0, c).tolist() == exp.tolist()
+
+
+def test_reference_binary_search_program(trtc):
+    # python/test/test_binary_search.py inputs; expected values are numpy's searchsorted
+    d_input = trtc.device_vector_from_list([0, 2, 5, 7, 8], "int32_t")
+    a = np.array([0, 2, 5, 7, 8])
+    qs = [0, 1, 2, 3, 8, 9]
+    assert [trtc.Lower_Bound(d_input, trtc.DVInt32(q)) for q in qs] == np.searchsorted(a, qs, "left").tolist()
+    assert [trtc.Upper_Bound(d_input, trtc.DVInt32(q)) for q in qs] == np.searchsorted(a, qs, "right").tolist()
+    assert [trtc.Binary_Search(d_input, trtc.DVInt32(q)) for q in qs] == [q in a for q in qs]
+    d_values = trtc.device_vector_from_list(qs, "int32_t")
+    d_output = trtc.device_vector("int32_t", 6)
+    trtc.Lower_Bound_V(d_input, d_values, d_output)
+    assert d_output.to_host().tolist() == [0, 1, 1, 2, 4, 5]
+    trtc.Upper_Bound_V(d_input, d_values, d_output)
+    assert d_output.to_host().tolist() == [1, 1, 2, 2, 5, 5]
+    trtc.Binary_Search_V(d_input, d_values, d_output)
+    assert d_output.to_host().tolist() == [1, 0, 1, 0, 1, 0]
+
+
+def test_vectorised_searches_large_and_comparator(trtc):
+    rng = np.random.default_rng(21)
+    a = np.sort(rng.integers(0, 10**6, 1 << 20)).astype(np.int64)
+    q = rng.integers(-10, 10**6 + 10, 300001).astype(np.int64)
+    da, dq = trtc.device_vector_from_numpy(a), trtc.device_vector_from_numpy(q)
+    out = trtc.device_vector("uint64_t", len(q))
+    trtc.Lower_Bound_V(da, dq, out)
+    assert np.array_equal(out.to_host(), np.searchsorted(a, q, "left").astype(np.uint64))
+    trtc.Upper_Bound_V(da, dq, out)
+    assert np.array_equal(out.to_host(), np.searchsorted(a, q, "right").astype(np.uint64))
+    found = trtc.device_vector("bool", len(q))
+    trtc.Binary_Search_V(da, dq, found)
+    assert np.array_equal(found.to_host().astype(bool), np.isin(q, a))
+    # descending order with Greater
+    d = a[::-1].copy()
+    dd = trtc.device_vector_from_numpy(d)
+    trtc.Lower_Bound_V(dd, dq, out, trtc.Greater())
+    exp = len(d) - np.searchsorted(a, q, "right")
+    assert np.array_equal(out.to_host(), exp.astype(np.uint64))
+    assert trtc.Lower_Bound(dd, trtc.DVInt64(int(q[0])), trtc.Greater()) == int(exp[0])

@@ -74,6 +74,9 @@ _SIGS = {
     "n_reduce": (vp, [vp, vp, vp]),
     "n_reduce_by_key": (u32, [vp, vp, vp, vp, vp, vp]),
     "n_min_element": (u64, [vp, vp]),
+    "n_lower_bound": (u64, [vp, vp, vp]), "n_upper_bound": (u64, [vp, vp, vp]),
+    "n_binary_search": (i32, [vp, vp, vp]), "n_lower_bound_v": (i32, [vp, vp, vp, vp]),
+    "n_upper_bound_v": (i32, [vp, vp, vp, vp]), "n_binary_search_v": (i32, [vp, vp, vp, vp]),
     "n_transform_reduce": (vp, [vp, vp, vp, vp]),
     "n_inclusive_scan": (i32, [vp, vp, vp]),
     "n_exclusive_scan": (i32, [vp, vp, vp, vp]),
@@ -556,6 +559,32 @@ def Transform_Reduce(vec, unary_op, value_init, binary_op):
 
 def Min_Element(vec, comp=None):
     return check_ull(lib.n_min_element(vec.m_cptr, _p(comp)))
+
+
+# ---------------------------------------------------------------- searches (Searching.py:30-84)
+def Lower_Bound(vec, value, comp=None):
+    return check_ull(lib.n_lower_bound(vec.m_cptr, value.m_cptr, _p(comp)))
+
+
+def Upper_Bound(vec, value, comp=None):
+    return check_ull(lib.n_upper_bound(vec.m_cptr, value.m_cptr, _p(comp)))
+
+
+def Binary_Search(vec, value, comp=None):
+    res = check_i(lib.n_binary_search(vec.m_cptr, value.m_cptr, _p(comp)))
+    return res != 0
+
+
+def Lower_Bound_V(vec, values, result, comp=None):
+    check_i(lib.n_lower_bound_v(vec.m_cptr, values.m_cptr, result.m_cptr, _p(comp)))
+
+
+def Upper_Bound_V(vec, values, result, comp=None):
+    check_i(lib.n_upper_bound_v(vec.m_cptr, values.m_cptr, result.m_cptr, _p(comp)))
+
+
+def Binary_Search_V(vec, values, result, comp=None):
+    check_i(lib.n_binary_search_v(vec.m_cptr, values.m_cptr, result.m_cptr, _p(comp)))
 
 
 def Copy_If(vec_in, vec_out, pred):

@@ -170,7 +170,8 @@ __global__ void __launch_bounds__(BLOCK, 4) compact2_kernel(InV in, StV stencil,
     auto vsel = [&](const E& x) -> bool {
         if constexpr (MODE == CM_PRED) return (bool)pred(x);
         else if constexpr (MODE == CM_NOT_EQUAL) return !(x == value);
-        else return !(bool)pred(x);
+        else if constexpr (MODE == CM_NOT_PRED) return !(bool)pred(x);
+        else return false;  // not used (VECOK excludes the other modes)
     };
 
     auto claim = [&]() -> size_t {

@@ -233,6 +233,34 @@ TRTC_EXPORT unsigned long long n_min_element(void* vec, void* comp) {
     size_t id = 0;
     return TRTC_Min_Element(V(vec), id) ? (unsigned long long)id : ~0ull;
 }
+// searches -- python/api_Searching.cpp:110-245 (NULL comparator = Less)
+TRTC_EXPORT unsigned long long n_lower_bound(void* vec, void* value, void* comp) {
+    size_t r = 0;
+    const bool ok = comp ? TRTC_Lower_Bound(V(vec), D(value), F(comp), r) : TRTC_Lower_Bound(V(vec), D(value), r);
+    return ok ? (unsigned long long)r : ~0ull;
+}
+TRTC_EXPORT unsigned long long n_upper_bound(void* vec, void* value, void* comp) {
+    size_t r = 0;
+    const bool ok = comp ? TRTC_Upper_Bound(V(vec), D(value), F(comp), r) : TRTC_Upper_Bound(V(vec), D(value), r);
+    return ok ? (unsigned long long)r : ~0ull;
+}
+TRTC_EXPORT int n_binary_search(void* vec, void* value, void* comp) {
+    bool r = false;
+    const bool ok = comp ? TRTC_Binary_Search(V(vec), D(value), F(comp), r) : TRTC_Binary_Search(V(vec), D(value), r);
+    return ok ? (r ? 1 : 0) : -1;
+}
+TRTC_EXPORT int n_lower_bound_v(void* vec, void* values, void* result, void* comp) {
+    return (comp ? TRTC_Lower_Bound_V(V(vec), V(values), V(result), F(comp))
+                 : TRTC_Lower_Bound_V(V(vec), V(values), V(result))) ? 0 : -1;
+}
+TRTC_EXPORT int n_upper_bound_v(void* vec, void* values, void* result, void* comp) {
+    return (comp ? TRTC_Upper_Bound_V(V(vec), V(values), V(result), F(comp))
+                 : TRTC_Upper_Bound_V(V(vec), V(values), V(result))) ? 0 : -1;
+}
+TRTC_EXPORT int n_binary_search_v(void* vec, void* values, void* result, void* comp) {
+    return (comp ? TRTC_Binary_Search_V(V(vec), V(values), V(result), F(comp))
+                 : TRTC_Binary_Search_V(V(vec), V(values), V(result))) ? 0 : -1;
+}
 TRTC_EXPORT void* n_transform_reduce(void* vec, void* uop, void* init, void* bop) {
     ViewBuf ret;
     if (!TRTC_Transform_Reduce(V(vec), F(uop), D(init), F(bop), ret)) return nullptr;

@@ -792,3 +792,87 @@ bool TRTC_Sort_By_Key(DVVectorLike& keys, DVVectorLike& values) {
     Functor less("Less");
     return sort_impl(keys, &values, less);
 }
+
+// ====================================================================== searches
+// binary_search.h: single values return through the host (one blocking copy, like the
+// reference's), vectorised searches write `result` (one thread per value).
+static bool search_value(int kind, const DVVectorLike& vec, const DeviceViewable& value, const Functor& comp,
+                         unsigned long long& out) {
+    if (vec.size() == 0) { out = 0; return true; }  // binary_search.cpp:27-31
+    if (!ensure_device()) return false;
+    const ViewArg vv = view_arg(vec);
+    ViewBuf vb;
+    std::string vt = vec.name_elem_cls();
+    if (!convert_scalar(value, vt, vb)) { vt = value.name_view_cls(); vb = value.view(); }
+    unsigned long long* d = (unsigned long long*)tmp_alloc(8, S());
+    if (!d) return false;
+    const std::string k = "trtc::search_one_kernel<" + num(kind) + ", " + vv.type + ", " + vt + ", " +
+                          comp.name_view_cls() + ">";
+    bool ok = jit_run({"trtc_search.cuh"}, k, 1, 32, {vv.bytes, vb, comp.view(), pod_bytes<unsigned long long*>(d)}) &&
+              TRTC_CUDA(cudaMemcpyAsync(&out, d, 8, cudaMemcpyDeviceToHost, S())) &&
+              check_device_errors(S(), "search");
+    tmp_free(d, S());
+    return ok;
+}
+
+static bool search_vector(int kind, const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result,
+                          const Functor& comp) {
+    const size_t m = values.size();
+    if (m == 0) return true;
+    if (!ensure_device()) return false;
+    const ViewArg vv = view_arg(vec), qv = view_arg(values), rv = view_arg(result);
+    const std::string k = "trtc::search_v_kernel<" + num(kind) + ", " + vv.type + ", " + qv.type + ", " + rv.type +
+                          ", " + comp.name_view_cls() + ">";
+    return jit_run({"trtc_search.cuh"}, k, grid_for(m, 256), 256,
+                   {vv.bytes, qv.bytes, rv.bytes, pod_bytes<size_t>(m), comp.view()});
+}
+
+bool TRTC_Lower_Bound(const DVVectorLike& vec, const DeviceViewable& value, const Functor& comp, size_t& result) {
+    unsigned long long r = 0;
+    if (!search_value(0, vec, value, comp, r)) return false;
+    result = (size_t)r;
+    return true;
+}
+bool TRTC_Lower_Bound(const DVVectorLike& vec, const DeviceViewable& value, size_t& result) {
+    return TRTC_Lower_Bound(vec, value, Functor("Less"), result);
+}
+bool TRTC_Upper_Bound(const DVVectorLike& vec, const DeviceViewable& value, const Functor& comp, size_t& result) {
+    unsigned long long r = 0;
+    if (!search_value(1, vec, value, comp, r)) return false;
+    result = (size_t)r;
+    return true;
+}
+bool TRTC_Upper_Bound(const DVVectorLike& vec, const DeviceViewable& value, size_t& result) {
+    return TRTC_Upper_Bound(vec, value, Functor("Less"), result);
+}
+bool TRTC_Binary_Search(const DVVectorLike& vec, const DeviceViewable& value, const Functor& comp, bool& result) {
+    unsigned long long r = 0;
+    if (vec.size() == 0) { result = false; return true; }
+    if (!search_value(2, vec, value, comp, r)) return false;
+    result = r != 0;
+    return true;
+}
+bool TRTC_Binary_Search(const DVVectorLike& vec, const DeviceViewable& value, bool& result) {
+    return TRTC_Binary_Search(vec, value, Functor("Less"), result);
+}
+bool TRTC_Lower_Bound_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result,
+                        const Functor& comp) {
+    return search_vector(0, vec, values, result, comp);
+}
+bool TRTC_Lower_Bound_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result) {
+    return search_vector(0, vec, values, result, Functor("Less"));
+}
+bool TRTC_Upper_Bound_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result,
+                        const Functor& comp) {
+    return search_vector(1, vec, values, result, comp);
+}
+bool TRTC_Upper_Bound_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result) {
+    return search_vector(1, vec, values, result, Functor("Less"));
+}
+bool TRTC_Binary_Search_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result,
+                          const Functor& comp) {
+    return search_vector(2, vec, values, result, comp);
+}
+bool TRTC_Binary_Search_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result) {
+    return search_vector(2, vec, values, result, Functor("Less"));
+}
