@@ -101,6 +101,11 @@ void* n_dvdiscard_create(const char* elem_cls, unsigned long long size);
 void* n_dvpermutation_create(void* ptr_value, void* ptr_index);
 void* n_dvreverse_create(void* ptr_value);
 void* n_dvtransform_create(void* ptr_in, const char* elem_cls, void* ptr_op);
+/* python/api.h:87,96-97 */
+void* n_dvtuple_create(void* ptr_dvs, void* ptr_names);
+void* n_dvzipped_create(void* ptr_vecs, void* ptr_elem_names);
+void* n_dvcustomvector_create(void* ptr_dvs, void* ptr_names, const char* name_idx, const char* body,
+                              const char* elem_cls, unsigned long long size, unsigned read_only);
 
 /* functors -- python/api.h:99-101 */
 void* n_functor_create(void* ptr_dvs, void* ptr_names, void* ptr_functor_params, const char* code_body);

@@ -254,6 +254,50 @@ private:
     size_t m_off[2];
 };
 
+// A struct of named device-viewable objects (DVTuple.h) -- its view struct has one member
+// per object, in order.
+class THRUST_RTC_API DVTuple : public DeviceViewable {
+public:
+    DVTuple(const std::vector<CapturedDeviceViewable>& elem_map);
+    virtual ViewBuf view() const;
+
+private:
+    std::vector<ViewBuf> m_view_elems;
+    std::vector<size_t> m_offsets;
+};
+
+// Vectors of equal length seen as one vector of structs (fake_vectors/DVZipped.h): element
+// i is { vecs[0][i], vecs[1][i], ... } under the given member names; writable when all are.
+class THRUST_RTC_API DVZipped : public DVVectorLike {
+public:
+    DVZipped(const std::vector<DVVectorLike*>& vecs, const std::vector<const char*>& elem_names);
+    virtual ViewBuf view() const;
+    virtual bool is_readable() const { return m_readable; }
+    virtual bool is_writable() const { return m_writable; }
+
+private:
+    bool m_readable = true, m_writable = true;
+    std::vector<ViewBuf> m_view_elems;
+    std::vector<size_t> m_offsets;
+};
+
+// A vector whose element idx is computed by user code over captured objects
+// (fake_vectors/DVCustomVector.h); read_only = false makes the code return a reference.
+class THRUST_RTC_API DVCustomVector : public DVVectorLike {
+public:
+    DVCustomVector(const std::vector<CapturedDeviceViewable>& arg_map, const char* name_idx, const char* code_body,
+                   const char* elem_cls, size_t size, bool read_only = true);
+    virtual ViewBuf view() const;
+    virtual bool is_writable() const { return !m_read_only; }
+
+private:
+    size_t m_size_val;
+    bool m_read_only;
+    std::vector<ViewBuf> m_view_args;
+    std::vector<size_t> m_arg_offsets;
+    size_t m_op_offset = 0, m_op_size = 0;
+};
+
 class THRUST_RTC_API Functor : public DeviceViewable {
 public:
     Functor(const std::vector<CapturedDeviceViewable>& arg_map, const std::vector<const char*>& functor_params,

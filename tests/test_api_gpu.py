@@ -351,3 +351,47 @@ def test_vectorised_searches_large_and_comparator(trtc):
     exp = len(d) - np.searchsorted(a, q, "right")
     assert np.array_equal(out.to_host(), exp.astype(np.uint64))
     assert trtc.Lower_Bound(dd, trtc.DVInt64(int(q[0])), trtc.Greater()) == int(exp[0])
+
+
+def test_reference_zipped_program(trtc):
+    # python/test/test_zipped.py with its outputs checked
+    d_int_in = trtc.device_vector_from_list([0, 1, 2, 3, 4], "int32_t")
+    d_float_in = trtc.device_vector_from_list([0.0, 10.0, 20.0, 30.0, 40.0], "float")
+    d_int_out = trtc.device_vector("int32_t", 5)
+    d_float_out = trtc.device_vector("float", 5)
+    zipped_in = trtc.DVZipped([d_int_in, d_float_in], ["a", "b"])
+    zipped_out = trtc.DVZipped([d_int_out, d_float_out], ["a", "b"])
+    trtc.Copy(zipped_in, zipped_out)
+    assert d_int_out.to_host().tolist() == [0, 1, 2, 3, 4]
+    assert d_float_out.to_host().tolist() == [0.0, 10.0, 20.0, 30.0, 40.0]
+    d_int_in = trtc.DVCounter(trtc.DVInt32(0), 5)
+    d_float_in = trtc.DVTransform(d_int_in, "float", trtc.Functor({}, ["i"], "        return (float)i*10.0f +10.0f;\n"))
+    zipped_in = trtc.DVZipped([d_int_in, d_float_in], ["a", "b"])
+    trtc.Copy(zipped_in, zipped_out)
+    assert d_int_out.to_host().tolist() == [0, 1, 2, 3, 4]
+    assert d_float_out.to_host().tolist() == [10.0, 20.0, 30.0, 40.0, 50.0]
+    const_in = trtc.DVConstant(trtc.DVTuple({"a": trtc.DVInt32(123), "b": trtc.DVFloat(456.0)}), 5)
+    trtc.Copy(const_in, zipped_out)
+    assert d_int_out.to_host().tolist() == [123] * 5
+    assert d_float_out.to_host().tolist() == [456.0] * 5
+
+
+def test_sort_by_key_zipped_payload_and_custom_vector(trtc):
+    # k-means demo pattern: Sort_By_Key with a zipped (x, y) payload
+    rng = np.random.default_rng(31)
+    n = 100_003
+    k = rng.integers(0, 97, n).astype(np.int32)
+    x = rng.standard_normal(n).astype(np.float32)
+    y = rng.standard_normal(n).astype(np.float32)
+    dk, dx, dy = (trtc.device_vector_from_numpy(a) for a in (k, x, y))
+    trtc.Sort_By_Key(dk, trtc.DVZipped([dx, dy], ["x", "y"]))
+    p = O.sort_perm(k)
+    assert dk.to_host().tolist() == k[p].tolist()
+    assert dx.to_host().tobytes() == x[p].tobytes() and dy.to_host().tobytes() == y[p].tobytes()
+    # a read-only custom vector feeding a reduction and a scan
+    src = trtc.device_vector_from_numpy(np.arange(1000, dtype=np.int32))
+    cv = trtc.DVCustomVector({"src": src}, "idx", "        return src[idx] * 2;\n", "int32_t", 1000)
+    assert trtc.Reduce(cv) == 2 * sum(range(1000))
+    out = trtc.device_vector("int32_t", 1000)
+    trtc.Inclusive_Scan(cv, out)
+    assert out.to_host().tolist() == np.cumsum(2 * np.arange(1000)).tolist()

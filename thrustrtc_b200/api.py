@@ -68,6 +68,8 @@ _SIGS = {
     "n_dvpermutation_create": (vp, [vp, vp]),
     "n_dvreverse_create": (vp, [vp]),
     "n_dvtransform_create": (vp, [vp, cstr, vp]),
+    "n_dvtuple_create": (vp, [vp, vp]), "n_dvzipped_create": (vp, [vp, vp]),
+    "n_dvcustomvector_create": (vp, [vp, vp, cstr, cstr, cstr, u64, u32]),
     "n_functor_create": (vp, [vp, vp, vp, cstr]),
     "n_built_in_functor_create": (vp, [cstr]),
     "n_copy": (i32, [vp, vp]),
@@ -462,6 +464,37 @@ class DVTransform(DVVectorLike):
     def __init__(self, vec_in, elem_cls, op):
         self.m_in, self.m_op = vec_in, op
         self.m_cptr = check_cptr(lib.n_dvtransform_create(vec_in.m_cptr, elem_cls.encode("utf-8"), op.m_cptr))
+
+
+class DVZipped(DVVectorLike):
+    """FakeVectors.py:37-42"""
+
+    def __init__(self, vecs, elem_names):
+        self.m_vecs = vecs
+        o_vecs, o_names = _ObjArray(vecs), _StrArray(elem_names)
+        self.m_cptr = check_cptr(lib.n_dvzipped_create(o_vecs.m_cptr, o_names.m_cptr))
+
+
+class DVCustomVector(DVVectorLike):
+    """FakeVectors.py:44-55"""
+
+    def __init__(self, arg_map, name_idx, code_body, elem_cls, size=-1, read_only=True):
+        self.m_arg_map = arg_map
+        o_names = _StrArray(list(arg_map.keys()))
+        o_elems = _ObjArray(list(arg_map.values()))
+        self.m_cptr = check_cptr(lib.n_dvcustomvector_create(
+            o_elems.m_cptr, o_names.m_cptr, name_idx.encode("utf-8"), code_body.encode("utf-8"),
+            elem_cls.encode("utf-8"), ctypes.c_ulonglong(size).value, 1 if read_only else 0))
+
+
+class DVTuple(DeviceViewable):
+    """DVTuple.py:5-12"""
+
+    def __init__(self, elem_map):
+        self.m_elem_map = elem_map
+        o_names = _StrArray(list(elem_map.keys()))
+        o_elems = _ObjArray(list(elem_map.values()))
+        self.m_cptr = check_cptr(lib.n_dvtuple_create(o_elems.m_cptr, o_names.m_cptr))
 
 
 # ---------------------------------------------------------------- functors

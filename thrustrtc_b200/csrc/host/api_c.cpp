@@ -192,6 +192,40 @@ TRTC_EXPORT void* n_dvtransform_create(void* pin, const char* elem_cls, void* po
     return new DVTransform(*(DVVectorLike*)pin, elem_cls, *(Functor*)pop);
 }
 
+// DVTuple / DVZipped / DVCustomVector -- python/api_DVTuple.cpp:8-20, api_FakeVectors.cpp:52-81
+static std::vector<CapturedDeviceViewable> captured(void* ptr_dvs, void* ptr_names) {
+    PtrArray* dvs = (PtrArray*)ptr_dvs;
+    StrArray* names = (StrArray*)ptr_names;
+    std::vector<CapturedDeviceViewable> m(dvs->size());
+    for (size_t i = 0; i < dvs->size(); i++) {
+        m[i].obj_name = (*names)[i].c_str();
+        m[i].obj = (*dvs)[i];
+    }
+    return m;
+}
+TRTC_EXPORT void* n_dvtuple_create(void* ptr_dvs, void* ptr_names) {
+    if (((PtrArray*)ptr_dvs)->size() != ((StrArray*)ptr_names)->size()) {
+        trtc_host::set_error("dvtuple: number of objects and names differ");
+        return nullptr;
+    }
+    return new DVTuple(captured(ptr_dvs, ptr_names));
+}
+TRTC_EXPORT void* n_dvzipped_create(void* ptr_vecs, void* ptr_elem_names) {
+    PtrArray* a = (PtrArray*)ptr_vecs;
+    StrArray* names = (StrArray*)ptr_elem_names;
+    if (a->empty() || a->size() != names->size()) {
+        trtc_host::set_error("dvzipped: number of vectors and element names differ");
+        return nullptr;
+    }
+    std::vector<DVVectorLike*> vecs(a->size());
+    for (size_t i = 0; i < a->size(); i++) vecs[i] = (DVVectorLike*)(*a)[i];
+    return new DVZipped(vecs, c_strs(*names));
+}
+TRTC_EXPORT void* n_dvcustomvector_create(void* ptr_dvs, void* ptr_names, const char* name_idx, const char* body,
+                                          const char* elem_cls, unsigned long long size, unsigned read_only) {
+    return new DVCustomVector(captured(ptr_dvs, ptr_names), name_idx, body, elem_cls, (size_t)size, read_only != 0);
+}
+
 // ------------------------------------------------------------------ functors
 TRTC_EXPORT void* n_functor_create(void* ptr_dvs, void* ptr_names, void* ptr_functor_params, const char* code_body) {
     PtrArray* dvs = (PtrArray*)ptr_dvs;

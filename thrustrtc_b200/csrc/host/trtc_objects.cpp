@@ -330,3 +330,156 @@ ViewBuf Functor::view() const {
         memcpy(ret.data() + m_offsets[i], m_view_args[i].data(), m_view_args[i].size());
     return ret;
 }
+
+// ------------------------------------------------------------------ DVTuple
+// struct { V0 name0; V1 name1; ... } of the objects' views (DVTuple.cpp:4-19)
+DVTuple::DVTuple(const std::vector<CapturedDeviceViewable>& elem_map) {
+    std::string body;
+    StructLayout sl;
+    m_view_elems.resize(elem_map.size());
+    for (size_t i = 0; i < elem_map.size(); i++) {
+        body += std::string("    ") + elem_map[i].obj->name_view_cls() + " " + elem_map[i].obj_name + ";\n";
+        m_view_elems[i] = elem_map[i].obj->view();
+        sl.add(Layout{elem_map[i].obj->view_size(), elem_map[i].obj->view_align()});
+    }
+    m_name_view_cls = jit_add_struct(body);
+    m_offsets = sl.offsets;
+    const Layout l = sl.finish();
+    m_offsets.push_back(l.size);
+    m_view_size = l.size;
+    m_view_align = l.align;
+    layout_register(m_name_view_cls, l);
+}
+ViewBuf DVTuple::view() const {
+    ViewBuf ret(m_offsets.back(), 0);
+    for (size_t i = 0; i < m_view_elems.size(); i++)
+        memcpy(ret.data() + m_offsets[i], m_view_elems[i].data(), m_view_elems[i].size());
+    return ret;
+}
+
+// ------------------------------------------------------------------ DVZipped
+// The element struct has the same body text as a DVTuple of scalars with the same member
+// names and types, so both name the same struct (a DVConstant of such a tuple assigns to a
+// zipped vector, as in the reference).
+static std::string zipped_elem_struct(const std::vector<DVVectorLike*>& vecs, const std::vector<const char*>& names) {
+    std::string body;
+    StructLayout sl;
+    for (size_t i = 0; i < vecs.size(); i++) {
+        body += std::string("    ") + vecs[i]->name_elem_cls() + " " + names[i] + ";\n";
+        Layout l;
+        if (!layout_of(vecs[i]->name_elem_cls(), l)) l = Layout{vecs[i]->elem_size(), vecs[i]->elem_size()};
+        sl.add(l);
+    }
+    const std::string name = jit_add_struct(body);
+    layout_register(name, sl.finish());
+    return name;
+}
+
+// reference struct: members are the vectors' reference types; converts to the element
+// struct when all are readable, assigns from it when all are writable
+static std::string zipped_ref_struct(const std::vector<DVVectorLike*>& vecs, const std::vector<const char*>& names,
+                                     const std::string& elem_cls, bool& readable, bool& writable) {
+    readable = writable = true;
+    for (auto* v : vecs) {
+        readable = readable && v->is_readable();
+        writable = writable && v->is_writable();
+    }
+    std::string body;
+    for (size_t i = 0; i < vecs.size(); i++)
+        body += std::string("    ") + vecs[i]->name_ref_type() + " " + names[i] + ";\n";
+    if (readable) {
+        body += "    __device__ operator " + elem_cls + "()\n    {\n        return {";
+        for (size_t i = 0; i < vecs.size(); i++) body += std::string(names[i]) + (i + 1 < vecs.size() ? ", " : "");
+        body += "};\n    }\n";
+    }
+    if (writable) {
+        body += "    __device__ CurType& operator = (const " + elem_cls + "& in)\n    {\n";
+        for (size_t i = 0; i < vecs.size(); i++)
+            body += std::string("        this->") + names[i] + " = in." + names[i] + ";\n";
+        body += "        return *this;\n    }\n";
+    }
+    return jit_add_struct(body);
+}
+
+static std::string zipped_elem_cls_for(const std::vector<DVVectorLike*>& vecs, const std::vector<const char*>& names) {
+    return vecs.empty() ? std::string("char") : zipped_elem_struct(vecs, names);
+}
+
+DVZipped::DVZipped(const std::vector<DVVectorLike*>& vecs, const std::vector<const char*>& elem_names)
+    : DVVectorLike(zipped_elem_cls_for(vecs, elem_names).c_str(), "char", vecs.empty() ? 0 : vecs[0]->size()) {
+    m_ref_type = zipped_ref_struct(vecs, elem_names, m_elem_cls, m_readable, m_writable);
+    std::string body = "    typedef " + m_elem_cls + " value_t;\n    typedef " + m_ref_type + " ref_t;\n";
+    StructLayout sl;
+    m_view_elems.resize(vecs.size());
+    for (size_t i = 0; i < vecs.size(); i++) {
+        body += std::string("    ") + vecs[i]->name_view_cls() + " " + elem_names[i] + ";\n";
+        m_view_elems[i] = vecs[i]->view();
+        sl.add(Layout{vecs[i]->view_size(), vecs[i]->view_align()});
+    }
+    body += std::string("    __device__ size_t size() const\n    {\n        return ") + elem_names[0] +
+            ".size();\n    }\n";
+    body += "    __device__ ref_t operator [](size_t idx)\n    {\n        return {";
+    for (size_t i = 0; i < vecs.size(); i++)
+        body += std::string(elem_names[i]) + "[idx]" + (i + 1 < vecs.size() ? ", " : "");
+    body += "};\n    }\n";
+    m_name_view_cls = jit_add_struct(body);
+    m_offsets = sl.offsets;
+    const Layout l = sl.finish();
+    m_offsets.push_back(l.size);
+    m_view_size = l.size;
+    m_view_align = l.align;
+    layout_register(m_name_view_cls, l);
+}
+ViewBuf DVZipped::view() const {
+    ViewBuf ret(m_offsets.back(), 0);
+    for (size_t i = 0; i < m_view_elems.size(); i++)
+        memcpy(ret.data() + m_offsets[i], m_view_elems[i].data(), m_view_elems[i].size());
+    return ret;
+}
+
+// ------------------------------------------------------------------ DVCustomVector
+// functor struct { captured views; ref_t operator()(size_t idx) { code } } wrapped in a
+// view struct { size_t _size; F _op; size(); operator[](idx) -> _op(idx) }
+// (fake_vectors/DVCustomVector.cpp:5-38)
+DVCustomVector::DVCustomVector(const std::vector<CapturedDeviceViewable>& arg_map, const char* name_idx,
+                               const char* code_body, const char* elem_cls, size_t size, bool read_only)
+    : DVVectorLike(elem_cls, read_only ? elem_cls : (std::string(elem_cls) + "&").c_str(), size),
+      m_size_val(size), m_read_only(read_only) {
+    std::string fbody;
+    StructLayout fl;
+    m_view_args.resize(arg_map.size());
+    for (size_t i = 0; i < arg_map.size(); i++) {
+        fbody += std::string("    ") + arg_map[i].obj->name_view_cls() + " " + arg_map[i].obj_name + ";\n";
+        m_view_args[i] = arg_map[i].obj->view();
+        fl.add(Layout{arg_map[i].obj->view_size(), arg_map[i].obj->view_align()});
+    }
+    fbody += "    __device__ inline " + m_ref_type + " operator()(size_t " + name_idx + ")\n    {\n";
+    fbody += code_body;
+    fbody += "    }\n";
+    const std::string fname = jit_add_struct(fbody);
+    m_arg_offsets = fl.offsets;
+    const Layout fla = fl.finish();
+    m_arg_offsets.push_back(fla.size);
+    layout_register(fname, fla);
+    std::string body = "    typedef " + m_elem_cls + " value_t;\n    typedef " + m_ref_type + " ref_t;\n";
+    body += "    size_t _size;\n    " + fname + " _op;\n";
+    body += "    __device__ inline size_t size() const\n    {\n        return _size;\n    }\n";
+    body += "    __device__ ref_t operator [](size_t idx)\n    {\n        return _op(idx);\n    }\n";
+    m_name_view_cls = jit_add_struct(body);
+    StructLayout sl;
+    sl.add(Layout{8, 8});
+    m_op_offset = sl.add(fla);
+    m_op_size = fla.size;
+    const Layout l = sl.finish();
+    m_view_size = l.size;
+    m_view_align = l.align;
+    layout_register(m_name_view_cls, l);
+}
+ViewBuf DVCustomVector::view() const {
+    ViewBuf ret(m_view_size, 0);
+    const unsigned long long sz = m_size_val;
+    memcpy(ret.data(), &sz, 8);
+    for (size_t i = 0; i < m_view_args.size(); i++)
+        memcpy(ret.data() + m_op_offset + m_arg_offsets[i], m_view_args[i].data(), m_view_args[i].size());
+    return ret;
+}
