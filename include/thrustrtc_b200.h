@@ -164,6 +164,56 @@ unsigned n_partition_copy_stencil(void* ptr_vec_in, void* ptr_stencil, void* ptr
 int n_sort(void* ptr_vec, void* ptr_comp);
 int n_sort_by_key(void* ptr_keys, void* ptr_values, void* ptr_comp);
 
+/* transformations -- python/api.h:104-117 (0 on success, -1 on failure) */
+int n_fill(void* ptr_vec, void* ptr_value);
+int n_replace(void* ptr_vec, void* ptr_old_value, void* ptr_new_value);
+int n_replace_if(void* ptr_vec, void* p_pred, void* ptr_new_value);
+int n_replace_copy(void* ptr_in, void* ptr_out, void* ptr_old_value, void* ptr_new_value);
+int n_replace_copy_if(void* ptr_in, void* ptr_out, void* p_pred, void* ptr_new_value);
+int n_for_each(void* ptr_vec, void* ptr_f);
+int n_adjacent_difference(void* ptr_in, void* ptr_out, void* ptr_binary_op);
+int n_sequence(void* ptr_vec, void* ptr_value_init, void* ptr_value_step);
+int n_tabulate(void* ptr_vec, void* ptr_op);
+int n_transform(void* ptr_in, void* ptr_out, void* ptr_op);
+int n_transform_binary(void* ptr_in1, void* ptr_in2, void* ptr_out, void* ptr_op);
+int n_transform_if(void* ptr_in, void* ptr_out, void* ptr_op, void* ptr_pred);
+int n_transform_if_stencil(void* ptr_in, void* ptr_stencil, void* ptr_out, void* ptr_op, void* ptr_pred);
+int n_transform_binary_if_stencil(void* ptr_in1, void* ptr_in2, void* ptr_stencil, void* ptr_out, void* ptr_op,
+                                  void* ptr_pred);
+
+/* copying -- python/api.h:120-125 */
+int n_gather(void* ptr_map, void* ptr_in, void* ptr_out);
+int n_gather_if(void* ptr_map, void* ptr_stencil, void* ptr_in, void* ptr_out, void* ptr_pred);
+int n_scatter(void* ptr_in, void* ptr_map, void* ptr_out);
+int n_scatter_if(void* ptr_in, void* ptr_map, void* ptr_stencil, void* ptr_out, void* ptr_pred);
+int n_swap(void* ptr_vec1, void* ptr_vec2);
+
+/* reductions -- python/api.h:128-142 (booleans: 1 / 0, -1 on failure) */
+unsigned long long n_count(void* ptr_vec, void* ptr_value);
+unsigned long long n_count_if(void* ptr_vec, void* ptr_pred);
+int n_equal(void* ptr_vec1, void* ptr_vec2, void* ptr_binary_pred);
+unsigned long long n_max_element(void* ptr_vec, void* ptr_comp);
+int n_minmax_element(void* ptr_vec, void* ptr_comp, unsigned long long* ret);
+void* n_inner_product(void* ptr_vec1, void* ptr_vec2, void* ptr_init, void* ptr_binary_op1, void* ptr_binary_op2);
+int n_all_of(void* ptr_vec, void* ptr_pred);
+int n_any_of(void* ptr_vec, void* ptr_pred);
+int n_none_of(void* ptr_vec, void* ptr_pred);
+int n_is_partitioned(void* ptr_vec, void* ptr_pred);
+int n_is_sorted(void* ptr_vec, void* ptr_comp);
+
+/* searching -- python/api.h:171-182 (a missing index reads as the size) */
+long long n_find(void* ptr_vec, void* ptr_value);
+long long n_find_if(void* ptr_vec, void* ptr_pred);
+long long n_find_if_not(void* ptr_vec, void* ptr_pred);
+long long n_mismatch(void* ptr_vec1, void* ptr_vec2, void* ptr_pred);
+unsigned long long n_partition_point(void* ptr_vec, void* ptr_pred);
+unsigned long long n_is_sorted_until(void* ptr_vec, void* ptr_comp);
+
+/* merging -- python/api.h:184-186 */
+int n_merge(void* ptr_vec1, void* ptr_vec2, void* ptr_vec_out, void* ptr_comp);
+int n_merge_by_key(void* ptr_keys1, void* ptr_keys2, void* ptr_value1, void* ptr_value2, void* ptr_keys_out,
+                   void* ptr_value_out, void* ptr_comp);
+
 #ifdef __cplusplus
 }
 #endif

@@ -454,3 +454,85 @@ THRUST_RTC_API uint32_t TRTC_Partition_Copy(const DVVectorLike& vec_in, DVVector
 THRUST_RTC_API uint32_t TRTC_Partition_Copy_Stencil(const DVVectorLike& vec_in, const DVVectorLike& stencil,
                                                     DVVectorLike& vec_true, DVVectorLike& vec_false,
                                                     const Functor& pred);
+
+// the remaining algorithms -- fill.h, sequence.h, tabulate.h, transform.h, replace.h,
+// for_each.h, adjacent_difference.h, gather.h, scatter.h, swap.h, count.h, equal.h,
+// logical.h, extrema.h, inner_product.h, find.h, mismatch.h, partition.h, sort.h, merge.h
+THRUST_RTC_API bool TRTC_Fill(DVVectorLike& vec, const DeviceViewable& value);
+THRUST_RTC_API bool TRTC_Sequence(DVVectorLike& vec);
+THRUST_RTC_API bool TRTC_Sequence(DVVectorLike& vec, const DeviceViewable& value_init);
+THRUST_RTC_API bool TRTC_Sequence(DVVectorLike& vec, const DeviceViewable& value_init,
+                                  const DeviceViewable& value_step);
+THRUST_RTC_API bool TRTC_Tabulate(DVVectorLike& vec, const Functor& op);
+THRUST_RTC_API bool TRTC_For_Each(DVVectorLike& vec, const Functor& f);
+THRUST_RTC_API bool TRTC_Transform(const DVVectorLike& vec_in, DVVectorLike& vec_out, const Functor& op);
+THRUST_RTC_API bool TRTC_Transform_Binary(const DVVectorLike& vec_in1, const DVVectorLike& vec_in2,
+                                          DVVectorLike& vec_out, const Functor& op);
+THRUST_RTC_API bool TRTC_Transform_If(const DVVectorLike& vec_in, DVVectorLike& vec_out, const Functor& op,
+                                      const Functor& pred);
+THRUST_RTC_API bool TRTC_Transform_If_Stencil(const DVVectorLike& vec_in, const DVVectorLike& vec_stencil,
+                                              DVVectorLike& vec_out, const Functor& op, const Functor& pred);
+THRUST_RTC_API bool TRTC_Transform_Binary_If_Stencil(const DVVectorLike& vec_in1, const DVVectorLike& vec_in2,
+                                                     const DVVectorLike& vec_stencil, DVVectorLike& vec_out,
+                                                     const Functor& op, const Functor& pred);
+THRUST_RTC_API bool TRTC_Replace(DVVectorLike& vec, const DeviceViewable& old_value, const DeviceViewable& new_value);
+THRUST_RTC_API bool TRTC_Replace_If(DVVectorLike& vec, const Functor& pred, const DeviceViewable& new_value);
+THRUST_RTC_API bool TRTC_Replace_Copy(const DVVectorLike& vec_in, DVVectorLike& vec_out,
+                                      const DeviceViewable& old_value, const DeviceViewable& new_value);
+THRUST_RTC_API bool TRTC_Replace_Copy_If(const DVVectorLike& vec_in, DVVectorLike& vec_out, const Functor& pred,
+                                         const DeviceViewable& new_value);
+THRUST_RTC_API bool TRTC_Adjacent_Difference(const DVVectorLike& vec_in, DVVectorLike& vec_out);
+THRUST_RTC_API bool TRTC_Adjacent_Difference(const DVVectorLike& vec_in, DVVectorLike& vec_out,
+                                             const Functor& binary_op);
+THRUST_RTC_API bool TRTC_Gather(const DVVectorLike& vec_map, const DVVectorLike& vec_in, DVVectorLike& vec_out);
+THRUST_RTC_API bool TRTC_Gather_If(const DVVectorLike& vec_map, const DVVectorLike& vec_stencil,
+                                   const DVVectorLike& vec_in, DVVectorLike& vec_out);
+THRUST_RTC_API bool TRTC_Gather_If(const DVVectorLike& vec_map, const DVVectorLike& vec_stencil,
+                                   const DVVectorLike& vec_in, DVVectorLike& vec_out, const Functor& pred);
+THRUST_RTC_API bool TRTC_Scatter(const DVVectorLike& vec_in, const DVVectorLike& vec_map, DVVectorLike& vec_out);
+THRUST_RTC_API bool TRTC_Scatter_If(const DVVectorLike& vec_in, const DVVectorLike& vec_map,
+                                    const DVVectorLike& vec_stencil, DVVectorLike& vec_out);
+THRUST_RTC_API bool TRTC_Scatter_If(const DVVectorLike& vec_in, const DVVectorLike& vec_map,
+                                    const DVVectorLike& vec_stencil, DVVectorLike& vec_out, const Functor& pred);
+THRUST_RTC_API bool TRTC_Swap(DVVectorLike& vec1, DVVectorLike& vec2);
+
+THRUST_RTC_API bool TRTC_Count(const DVVectorLike& vec, const DeviceViewable& value, size_t& ret);
+THRUST_RTC_API bool TRTC_Count_If(const DVVectorLike& vec, const Functor& pred, size_t& ret);
+THRUST_RTC_API bool TRTC_Equal(const DVVectorLike& vec1, const DVVectorLike& vec2, bool& ret);
+THRUST_RTC_API bool TRTC_Equal(const DVVectorLike& vec1, const DVVectorLike& vec2, const Functor& binary_pred,
+                               bool& ret);
+THRUST_RTC_API bool TRTC_All_Of(const DVVectorLike& vec, const Functor& pred, bool& ret);
+THRUST_RTC_API bool TRTC_Any_Of(const DVVectorLike& vec, const Functor& pred, bool& ret);
+THRUST_RTC_API bool TRTC_None_Of(const DVVectorLike& vec, const Functor& pred, bool& ret);
+THRUST_RTC_API bool TRTC_Min_Element(const DVVectorLike& vec, const Functor& comp, size_t& id_min);
+THRUST_RTC_API bool TRTC_Max_Element(const DVVectorLike& vec, size_t& id_max);
+THRUST_RTC_API bool TRTC_Max_Element(const DVVectorLike& vec, const Functor& comp, size_t& id_max);
+THRUST_RTC_API bool TRTC_MinMax_Element(const DVVectorLike& vec, size_t& id_min, size_t& id_max);
+THRUST_RTC_API bool TRTC_MinMax_Element(const DVVectorLike& vec, const Functor& comp, size_t& id_min, size_t& id_max);
+THRUST_RTC_API bool TRTC_Inner_Product(const DVVectorLike& vec1, const DVVectorLike& vec2, const DeviceViewable& init,
+                                       ViewBuf& ret);
+THRUST_RTC_API bool TRTC_Inner_Product(const DVVectorLike& vec1, const DVVectorLike& vec2, const DeviceViewable& init,
+                                       ViewBuf& ret, const Functor& binary_op1, const Functor& binary_op2);
+
+THRUST_RTC_API bool TRTC_Find(const DVVectorLike& vec, const DeviceViewable& value, size_t& result);
+THRUST_RTC_API bool TRTC_Find_If(const DVVectorLike& vec, const Functor& pred, size_t& result);
+THRUST_RTC_API bool TRTC_Find_If_Not(const DVVectorLike& vec, const Functor& pred, size_t& result);
+THRUST_RTC_API bool TRTC_Mismatch(const DVVectorLike& vec1, const DVVectorLike& vec2, size_t& result);
+THRUST_RTC_API bool TRTC_Mismatch(const DVVectorLike& vec1, const DVVectorLike& vec2, const Functor& pred,
+                                  size_t& result);
+THRUST_RTC_API bool TRTC_Partition_Point(const DVVectorLike& vec, const Functor& pred, size_t& result);
+THRUST_RTC_API bool TRTC_Is_Partitioned(const DVVectorLike& vec, const Functor& pred, bool& result);
+THRUST_RTC_API bool TRTC_Is_Sorted(const DVVectorLike& vec, bool& result);
+THRUST_RTC_API bool TRTC_Is_Sorted(const DVVectorLike& vec, const Functor& comp, bool& result);
+THRUST_RTC_API bool TRTC_Is_Sorted_Until(const DVVectorLike& vec, size_t& result);
+THRUST_RTC_API bool TRTC_Is_Sorted_Until(const DVVectorLike& vec, const Functor& comp, size_t& result);
+
+THRUST_RTC_API bool TRTC_Merge(const DVVectorLike& vec1, const DVVectorLike& vec2, DVVectorLike& vec_out);
+THRUST_RTC_API bool TRTC_Merge(const DVVectorLike& vec1, const DVVectorLike& vec2, DVVectorLike& vec_out,
+                               const Functor& comp);
+THRUST_RTC_API bool TRTC_Merge_By_Key(const DVVectorLike& keys1, const DVVectorLike& keys2,
+                                      const DVVectorLike& value1, const DVVectorLike& value2, DVVectorLike& keys_out,
+                                      DVVectorLike& value_out);
+THRUST_RTC_API bool TRTC_Merge_By_Key(const DVVectorLike& keys1, const DVVectorLike& keys2,
+                                      const DVVectorLike& value1, const DVVectorLike& value2, DVVectorLike& keys_out,
+                                      DVVectorLike& value_out, const Functor& comp);

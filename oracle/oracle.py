@@ -2,7 +2,8 @@
 
 This module restates, on the host, the results the reference library (fynv/ThrustRTC)
 produces for sort / scan / scan_by_key / reduce / min_element (C++ in trtc_oracle.cpp,
-loaded with ctypes) and for the scan-based compaction family (numpy, below).  It is the
+loaded with ctypes), for the scan-based compaction family and for the remaining algorithms
+(index trees of the extrema, merge ranks, first-index searches; numpy, below).  It is the
 checker for the CUDA kernels of ``thrustrtc_b200``: only ``tests/``,
 ``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference`` legs of
 ``bench.py`` may import it.  Nothing in the product package imports or calls it.
@@ -238,3 +239,87 @@ def reduce_by_key(keys, vals, op="Plus"):
     if len(keys) > 1:
         tail[:-1] = keys[:-1] != keys[1:]
     return keys[tail], s[tail]
+
+
+# ---------------------------------------------------------------- remaining algorithms (numpy)
+
+def index_tree(x, maximum=False, less=None):
+    """Max/Min_Element (extrema.cpp:5-44) over internal/general_reduce.cpp:55-95: blocks of 256
+    slots, s = 128..1, slot t takes op(h[t], h[t+s]) when t + s < L; rounds repeat on the
+    block results.  max: comp(v[i1], v[i2]) ? i2 : i1; min: comp(v[i2], v[i1]) ? i2 : i1.
+    `less(a, b)` is the elementwise comparison (default a < b, so NaN compares false)."""
+    x = np.asarray(x)
+    if len(x) == 0:
+        return None
+    if less is None:
+        less = lambda a, b: a < b  # noqa: E731
+    cur = np.arange(len(x), dtype=np.int64)
+    first = True
+    while first or len(cur) > 1:
+        first = False
+        m = len(cur)
+        nb = (m + 255) // 256
+        h = np.zeros(nb * 256, dtype=np.int64)
+        h[:m] = cur
+        h = h.reshape(nb, 256)
+        L = np.minimum(256, m - np.arange(nb) * 256)[:, None]
+        s = 128
+        while s > 0:
+            t = np.arange(s)[None, :]
+            ok = (t + s) < L
+            i1, i2 = h[:, :s], h[:, s:2 * s]
+            take2 = less(x[i1], x[i2]) if maximum else less(x[i2], x[i1])
+            h[:, :s] = np.where(ok & take2, i2, i1)
+            s >>= 1
+        cur = h[:, 0].copy()
+    return int(cur[0])
+
+
+def first_true(flags):
+    """internal/general_find.cpp:4-42: the lowest index whose flag is set, else None."""
+    idx = np.flatnonzero(np.asarray(flags, dtype=bool))
+    return int(idx[0]) if len(idx) else None
+
+
+def merge(a, b, va=None, vb=None, less=None):
+    """merge.cpp:3-66: a[i] goes to i + lower_bound(b, a[i]), b[j] to j + upper_bound(a, b[j])
+    under `less` (default <; pass lambda x, y: x > y for Greater).  Returns keys (, values)."""
+    a, b = np.asarray(a), np.asarray(b)
+    if less is None:
+        pa = np.arange(len(a)) + np.searchsorted(b, a, side="left")
+        pb = np.arange(len(b)) + np.searchsorted(a, b, side="right")
+    else:
+        pa = np.array([i + sum(1 for y in b if less(y, x)) for i, x in enumerate(a)], dtype=np.int64)
+        pb = np.array([j + sum(1 for x in a if not less(y, x)) for j, y in enumerate(b)], dtype=np.int64)
+    out = np.empty(len(a) + len(b), dtype=np.result_type(a, b))
+    out[pa], out[pb] = a, b
+    if va is None:
+        return out
+    vout = np.empty(len(a) + len(b), dtype=np.result_type(np.asarray(va), np.asarray(vb)))
+    vout[pa], vout[pb] = va, vb
+    return out, vout
+
+
+def adjacent_difference(x):
+    """adjacent_difference.cpp:3-13: out[0] = in[0], out[i] = in[i] - in[i-1] in the element type."""
+    x = np.asarray(x)
+    out = x.copy()
+    if len(x) > 1:
+        out[1:] = x[1:] - x[:-1]
+    return out
+
+
+def is_sorted_until(x, less=None):
+    """sort.cpp:93-103: the first i >= 1 with comp(v[i], v[i-1]), else the size."""
+    x = np.asarray(x)
+    if len(x) < 2:
+        return len(x)
+    brk = (x[1:] < x[:-1]) if less is None else less(x[1:], x[:-1])
+    i = first_true(brk)
+    return len(x) if i is None else i + 1
+
+
+def is_partitioned(flags):
+    """partition.cpp:199-214: no true flag right after a false one (true when empty)."""
+    f = np.asarray(flags, dtype=bool)
+    return not bool(np.any(~f[:-1] & f[1:])) if len(f) > 1 else True

@@ -117,3 +117,25 @@ def test_compaction_restatements():
     assert out.tolist() == [2, 4, 6, 8, 10, 1, 3, 5, 7, 9] and c == 5
     k, v = O.reduce_by_key(x, np.array([9, 8, 7, 6, 5, 4, 3], np.int32))
     assert k.tolist() == [1, 3, 2, 1] and v.tolist() == [9, 21, 9, 3]
+
+
+def test_remaining_algorithm_restatements():
+    # the numpy index tree agrees with the C++ restatement of extrema.cpp (NaNs included)
+    rng = np.random.default_rng(11)
+    for n in (1, 255, 256, 257, 70000):
+        x = rng.integers(0, 40, n).astype(np.float32)
+        x[rng.integers(0, n, max(1, n // 50))] = np.nan
+        assert O.index_tree(x) == O.min_element(x)
+    # hand-worked cases of python/test/test_extrema.py, test_merge.py, test_sort.py,
+    # test_partition.py, test_adjacent_difference.py (Thrust semantics)
+    assert O.index_tree([1, 0, 2, 2, 1, 3]) == 1 and O.index_tree([1, 0, 2, 2, 1, 3], maximum=True) == 5
+    assert O.merge([1, 3, 5, 7, 9, 11], [1, 1, 2, 3, 5, 8, 13]).tolist() == [1, 1, 1, 2, 3, 3, 5, 5, 7, 8, 9, 11, 13]
+    k, v = O.merge([11, 9, 7, 5, 3, 1], [13, 8, 5, 3, 2, 1, 1], [0] * 6, [1] * 7, less=lambda a, b: a > b)
+    assert k.tolist() == [13, 11, 9, 8, 7, 5, 5, 3, 3, 2, 1, 1, 1]
+    assert v.tolist() == [1, 0, 0, 1, 0, 0, 1, 0, 1, 1, 0, 1, 1]
+    assert O.is_sorted_until([0, 1, 2, 3, 0, 1, 2, 3]) == 4
+    assert O.is_sorted_until([3, 2, 1, 0, 3, 2, 1, 0], less=lambda a, b: a > b) == 4
+    assert O.is_partitioned(np.array([2, 4, 6, 8, 10, 1, 3, 5, 7, 9]) % 2 == 0)
+    assert not O.is_partitioned(np.arange(1, 11) % 2 == 0)
+    assert O.adjacent_difference(np.array([1, 2, 1, 2, 1, 2, 1, 2], np.int32)).tolist() == [1, 1, -1, 1, -1, 1, -1, 1]
+    assert O.first_true([False, False]) is None and O.first_true([0, 1, 1]) == 1

@@ -104,6 +104,35 @@ _SIGS = {
     "n_partition_copy_stencil": (u32, [vp, vp, vp, vp, vp]),
     "n_sort": (i32, [vp, vp]),
     "n_sort_by_key": (i32, [vp, vp, vp]),
+    "n_fill": (i32, [vp, vp]),
+    "n_replace": (i32, [vp, vp, vp]), "n_replace_if": (i32, [vp, vp, vp]),
+    "n_replace_copy": (i32, [vp, vp, vp, vp]), "n_replace_copy_if": (i32, [vp, vp, vp, vp]),
+    "n_for_each": (i32, [vp, vp]),
+    "n_adjacent_difference": (i32, [vp, vp, vp]),
+    "n_sequence": (i32, [vp, vp, vp]),
+    "n_tabulate": (i32, [vp, vp]),
+    "n_transform": (i32, [vp, vp, vp]),
+    "n_transform_binary": (i32, [vp, vp, vp, vp]),
+    "n_transform_if": (i32, [vp, vp, vp, vp]),
+    "n_transform_if_stencil": (i32, [vp, vp, vp, vp, vp]),
+    "n_transform_binary_if_stencil": (i32, [vp, vp, vp, vp, vp, vp]),
+    "n_gather": (i32, [vp, vp, vp]), "n_gather_if": (i32, [vp, vp, vp, vp, vp]),
+    "n_scatter": (i32, [vp, vp, vp]), "n_scatter_if": (i32, [vp, vp, vp, vp, vp]),
+    "n_swap": (i32, [vp, vp]),
+    "n_count": (u64, [vp, vp]), "n_count_if": (u64, [vp, vp]),
+    "n_equal": (i32, [vp, vp, vp]),
+    "n_max_element": (u64, [vp, vp]),
+    "n_minmax_element": (i32, [vp, vp, ctypes.POINTER(u64)]),
+    "n_inner_product": (vp, [vp, vp, vp, vp, vp]),
+    "n_all_of": (i32, [vp, vp]), "n_any_of": (i32, [vp, vp]), "n_none_of": (i32, [vp, vp]),
+    "n_is_partitioned": (i32, [vp, vp]),
+    "n_is_sorted": (i32, [vp, vp]),
+    "n_find": (i64, [vp, vp]), "n_find_if": (i64, [vp, vp]), "n_find_if_not": (i64, [vp, vp]),
+    "n_mismatch": (i64, [vp, vp, vp]),
+    "n_partition_point": (u64, [vp, vp]),
+    "n_is_sorted_until": (u64, [vp, vp]),
+    "n_merge": (i32, [vp, vp, vp, vp]),
+    "n_merge_by_key": (i32, [vp, vp, vp, vp, vp, vp, vp]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _fn = getattr(lib, _name)
@@ -684,3 +713,180 @@ def Partition_Copy(vec_in, vec_true, vec_false, pred):
 def Partition_Copy_Stencil(vec_in, stencil, vec_true, vec_false, pred):
     return check_u(lib.n_partition_copy_stencil(vec_in.m_cptr, stencil.m_cptr, vec_true.m_cptr, vec_false.m_cptr,
                                                 pred.m_cptr))
+
+
+# ---------------------------------------------------------------- transformations (Transformations.py)
+def Fill(vec, value):
+    check_i(lib.n_fill(vec.m_cptr, value.m_cptr))
+
+
+def Replace(vec, old_value, new_value):
+    check_i(lib.n_replace(vec.m_cptr, old_value.m_cptr, new_value.m_cptr))
+
+
+def Replace_If(vec, pred, new_value):
+    check_i(lib.n_replace_if(vec.m_cptr, pred.m_cptr, new_value.m_cptr))
+
+
+def Replace_Copy(vec_in, vec_out, old_value, new_value):
+    check_i(lib.n_replace_copy(vec_in.m_cptr, vec_out.m_cptr, old_value.m_cptr, new_value.m_cptr))
+
+
+def Replace_Copy_If(vec_in, vec_out, pred, new_value):
+    check_i(lib.n_replace_copy_if(vec_in.m_cptr, vec_out.m_cptr, pred.m_cptr, new_value.m_cptr))
+
+
+def For_Each(vec, f):
+    check_i(lib.n_for_each(vec.m_cptr, f.m_cptr))
+
+
+def Adjacent_Difference(vec_in, vec_out, binary_op=None):
+    check_i(lib.n_adjacent_difference(vec_in.m_cptr, vec_out.m_cptr, _p(binary_op)))
+
+
+def Sequence(vec, value_init=None, value_step=None):
+    check_i(lib.n_sequence(vec.m_cptr, _p(value_init), _p(value_step)))
+
+
+def Tabulate(vec, op):
+    check_i(lib.n_tabulate(vec.m_cptr, op.m_cptr))
+
+
+def Transform(vec_in, vec_out, op):
+    check_i(lib.n_transform(vec_in.m_cptr, vec_out.m_cptr, op.m_cptr))
+
+
+def Transform_Binary(vec_in1, vec_in2, vec_out, op):
+    check_i(lib.n_transform_binary(vec_in1.m_cptr, vec_in2.m_cptr, vec_out.m_cptr, op.m_cptr))
+
+
+def Transform_If(vec_in, vec_out, op, pred):
+    check_i(lib.n_transform_if(vec_in.m_cptr, vec_out.m_cptr, op.m_cptr, pred.m_cptr))
+
+
+def Transform_If_Stencil(vec_in, vec_stencil, vec_out, op, pred):
+    check_i(lib.n_transform_if_stencil(vec_in.m_cptr, vec_stencil.m_cptr, vec_out.m_cptr, op.m_cptr, pred.m_cptr))
+
+
+def Transform_Binary_If_Stencil(vec_in1, vec_in2, vec_stencil, vec_out, op, pred):
+    check_i(lib.n_transform_binary_if_stencil(vec_in1.m_cptr, vec_in2.m_cptr, vec_stencil.m_cptr, vec_out.m_cptr,
+                                              op.m_cptr, pred.m_cptr))
+
+
+# ---------------------------------------------------------------- copying (Copying.py)
+def Gather(vec_map, vec_in, vec_out):
+    check_i(lib.n_gather(vec_map.m_cptr, vec_in.m_cptr, vec_out.m_cptr))
+
+
+def Gather_If(vec_map, vec_stencil, vec_in, vec_out, pred=None):
+    check_i(lib.n_gather_if(vec_map.m_cptr, vec_stencil.m_cptr, vec_in.m_cptr, vec_out.m_cptr, _p(pred)))
+
+
+def Scatter(vec_in, vec_map, vec_out):
+    check_i(lib.n_scatter(vec_in.m_cptr, vec_map.m_cptr, vec_out.m_cptr))
+
+
+def Scatter_If(vec_in, vec_map, vec_stencil, vec_out, pred=None):
+    check_i(lib.n_scatter_if(vec_in.m_cptr, vec_map.m_cptr, vec_stencil.m_cptr, vec_out.m_cptr, _p(pred)))
+
+
+def Swap(vec1, vec2):
+    check_i(lib.n_swap(vec1.m_cptr, vec2.m_cptr))
+
+
+# ---------------------------------------------------------------- reductions (Reductions.py)
+def Count(vec, value):
+    return check_ull(lib.n_count(vec.m_cptr, value.m_cptr))
+
+
+def Count_If(vec, pred):
+    return check_ull(lib.n_count_if(vec.m_cptr, pred.m_cptr))
+
+
+def _bool(r):
+    return check_i(r) != 0
+
+
+def Equal(vec1, vec2, binary_pred=None):
+    return _bool(lib.n_equal(vec1.m_cptr, vec2.m_cptr, _p(binary_pred)))
+
+
+def Max_Element(vec, comp=None):
+    return check_ull(lib.n_max_element(vec.m_cptr, _p(comp)))
+
+
+def MinMax_Element(vec, comp=None):
+    arr = np.zeros(2, dtype=np.uint64)
+    check_i(lib.n_minmax_element(vec.m_cptr, _p(comp), arr.ctypes.data_as(ctypes.POINTER(u64))))
+    return (arr[0], arr[1])
+
+
+def Inner_Product(vec1, vec2, value_init, binary_op1=None, binary_op2=None):
+    dvptr = check_cptr(lib.n_inner_product(vec1.m_cptr, vec2.m_cptr, value_init.m_cptr, _p(binary_op1),
+                                           _p(binary_op2)))
+    ret = _value_from_dvptr(dvptr)
+    lib.n_dv_destroy(dvptr)
+    return ret
+
+
+def All_Of(vec, pred):
+    return _bool(lib.n_all_of(vec.m_cptr, _p(pred)))
+
+
+def Any_Of(vec, pred):
+    return _bool(lib.n_any_of(vec.m_cptr, _p(pred)))
+
+
+def None_Of(vec, pred):
+    return _bool(lib.n_none_of(vec.m_cptr, _p(pred)))
+
+
+def Is_Partitioned(vec, pred):
+    return _bool(lib.n_is_partitioned(vec.m_cptr, pred.m_cptr))
+
+
+def Is_Sorted(vec, comp=None):
+    return _bool(lib.n_is_sorted(vec.m_cptr, _p(comp)))
+
+
+# ---------------------------------------------------------------- searching (Searching.py)
+def _index(r, size):
+    r = check_i(r)
+    return None if r >= size else r
+
+
+def Find(vec, value):
+    return _index(lib.n_find(vec.m_cptr, value.m_cptr), vec.size())
+
+
+def Find_If(vec, pred):
+    return _index(lib.n_find_if(vec.m_cptr, pred.m_cptr), vec.size())
+
+
+def Find_If_Not(vec, pred):
+    return _index(lib.n_find_if_not(vec.m_cptr, pred.m_cptr), vec.size())
+
+
+def Mismatch(vec1, vec2, pred=None):
+    r = check_i(lib.n_mismatch(vec1.m_cptr, vec2.m_cptr, _p(pred)))
+    if r >= vec1.size() and r >= vec2.size():
+        return None
+    return r
+
+
+def Partition_Point(vec, pred):
+    return check_ull(lib.n_partition_point(vec.m_cptr, pred.m_cptr))
+
+
+def Is_Sorted_Until(vec, comp=None):
+    return check_ull(lib.n_is_sorted_until(vec.m_cptr, _p(comp)))
+
+
+# ---------------------------------------------------------------- merging (Merging.py)
+def Merge(vec1, vec2, vec_out, comp=None):
+    check_i(lib.n_merge(vec1.m_cptr, vec2.m_cptr, vec_out.m_cptr, _p(comp)))
+
+
+def Merge_By_Key(keys1, keys2, value1, value2, keys_out, value_out, comp=None):
+    check_i(lib.n_merge_by_key(keys1.m_cptr, keys2.m_cptr, value1.m_cptr, value2.m_cptr, keys_out.m_cptr,
+                               value_out.m_cptr, _p(comp)))

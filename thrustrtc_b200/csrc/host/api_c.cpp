@@ -260,12 +260,9 @@ TRTC_EXPORT unsigned n_reduce_by_key(void* ki, void* vi, void* ko, void* vo, voi
     return TRTC_Reduce_By_Key(V(ki), V(vi), V(ko), V(vo), F(pred), F(op));
 }
 TRTC_EXPORT unsigned long long n_min_element(void* vec, void* comp) {
-    if (comp && !(F(comp).is_built_in() && F(comp).name_view_cls() == "Less")) {
-        trtc_host::set_error("min_element: only the default Less comparison is provided");
-        return ~0ull;
-    }
     size_t id = 0;
-    return TRTC_Min_Element(V(vec), id) ? (unsigned long long)id : ~0ull;
+    const bool ok = comp ? TRTC_Min_Element(V(vec), F(comp), id) : TRTC_Min_Element(V(vec), id);
+    return ok ? (unsigned long long)id : ~0ull;
 }
 // searches -- python/api_Searching.cpp:110-245 (NULL comparator = Less)
 TRTC_EXPORT unsigned long long n_lower_bound(void* vec, void* value, void* comp) {
@@ -381,4 +378,150 @@ TRTC_EXPORT int n_sort(void* vec, void* comp) {
 }
 TRTC_EXPORT int n_sort_by_key(void* keys, void* values, void* comp) {
     return (comp ? TRTC_Sort_By_Key(V(keys), V(values), F(comp)) : TRTC_Sort_By_Key(V(keys), V(values))) ? 0 : -1;
+}
+
+// ---- the remaining entry points (python/api.h:104-186); return conventions of the
+// reference's python/api_*.cpp: 0 / -1 for int status, 1 / 0 / -1 for booleans,
+// (unsigned long long)-1 for failed counts and indices, NULL for failed value results.
+// transformations -- python/api_Transformations.cpp
+TRTC_EXPORT int n_fill(void* vec, void* value) { return TRTC_Fill(V(vec), D(value)) ? 0 : -1; }
+TRTC_EXPORT int n_replace(void* vec, void* old_value, void* new_value) {
+    return TRTC_Replace(V(vec), D(old_value), D(new_value)) ? 0 : -1;
+}
+TRTC_EXPORT int n_replace_if(void* vec, void* pred, void* new_value) {
+    return TRTC_Replace_If(V(vec), F(pred), D(new_value)) ? 0 : -1;
+}
+TRTC_EXPORT int n_replace_copy(void* in, void* out, void* old_value, void* new_value) {
+    return TRTC_Replace_Copy(V(in), V(out), D(old_value), D(new_value)) ? 0 : -1;
+}
+TRTC_EXPORT int n_replace_copy_if(void* in, void* out, void* pred, void* new_value) {
+    return TRTC_Replace_Copy_If(V(in), V(out), F(pred), D(new_value)) ? 0 : -1;
+}
+TRTC_EXPORT int n_for_each(void* vec, void* f) { return TRTC_For_Each(V(vec), F(f)) ? 0 : -1; }
+TRTC_EXPORT int n_adjacent_difference(void* in, void* out, void* op) {
+    return (op ? TRTC_Adjacent_Difference(V(in), V(out), F(op)) : TRTC_Adjacent_Difference(V(in), V(out))) ? 0 : -1;
+}
+TRTC_EXPORT int n_sequence(void* vec, void* init, void* step) {
+    bool ok;
+    if (!init) ok = TRTC_Sequence(V(vec));
+    else if (!step) ok = TRTC_Sequence(V(vec), D(init));
+    else ok = TRTC_Sequence(V(vec), D(init), D(step));
+    return ok ? 0 : -1;
+}
+TRTC_EXPORT int n_tabulate(void* vec, void* op) { return TRTC_Tabulate(V(vec), F(op)) ? 0 : -1; }
+TRTC_EXPORT int n_transform(void* in, void* out, void* op) { return TRTC_Transform(V(in), V(out), F(op)) ? 0 : -1; }
+TRTC_EXPORT int n_transform_binary(void* in1, void* in2, void* out, void* op) {
+    return TRTC_Transform_Binary(V(in1), V(in2), V(out), F(op)) ? 0 : -1;
+}
+TRTC_EXPORT int n_transform_if(void* in, void* out, void* op, void* pred) {
+    return TRTC_Transform_If(V(in), V(out), F(op), F(pred)) ? 0 : -1;
+}
+TRTC_EXPORT int n_transform_if_stencil(void* in, void* st, void* out, void* op, void* pred) {
+    return TRTC_Transform_If_Stencil(V(in), V(st), V(out), F(op), F(pred)) ? 0 : -1;
+}
+TRTC_EXPORT int n_transform_binary_if_stencil(void* in1, void* in2, void* st, void* out, void* op, void* pred) {
+    return TRTC_Transform_Binary_If_Stencil(V(in1), V(in2), V(st), V(out), F(op), F(pred)) ? 0 : -1;
+}
+// copying -- python/api_Copying.cpp
+TRTC_EXPORT int n_gather(void* map, void* in, void* out) { return TRTC_Gather(V(map), V(in), V(out)) ? 0 : -1; }
+TRTC_EXPORT int n_gather_if(void* map, void* st, void* in, void* out, void* pred) {
+    return (pred ? TRTC_Gather_If(V(map), V(st), V(in), V(out), F(pred)) : TRTC_Gather_If(V(map), V(st), V(in), V(out)))
+               ? 0 : -1;
+}
+TRTC_EXPORT int n_scatter(void* in, void* map, void* out) { return TRTC_Scatter(V(in), V(map), V(out)) ? 0 : -1; }
+TRTC_EXPORT int n_scatter_if(void* in, void* map, void* st, void* out, void* pred) {
+    return (pred ? TRTC_Scatter_If(V(in), V(map), V(st), V(out), F(pred))
+                 : TRTC_Scatter_If(V(in), V(map), V(st), V(out))) ? 0 : -1;
+}
+TRTC_EXPORT int n_swap(void* vec1, void* vec2) { return TRTC_Swap(V(vec1), V(vec2)) ? 0 : -1; }
+// reductions -- python/api_Reductions.cpp
+TRTC_EXPORT unsigned long long n_count(void* vec, void* value) {
+    size_t r = 0;
+    return TRTC_Count(V(vec), D(value), r) ? (unsigned long long)r : ~0ull;
+}
+TRTC_EXPORT unsigned long long n_count_if(void* vec, void* pred) {
+    size_t r = 0;
+    return TRTC_Count_If(V(vec), F(pred), r) ? (unsigned long long)r : ~0ull;
+}
+TRTC_EXPORT int n_equal(void* vec1, void* vec2, void* pred) {
+    bool r = false;
+    const bool ok = pred ? TRTC_Equal(V(vec1), V(vec2), F(pred), r) : TRTC_Equal(V(vec1), V(vec2), r);
+    return ok ? (r ? 1 : 0) : -1;
+}
+TRTC_EXPORT unsigned long long n_max_element(void* vec, void* comp) {
+    size_t id = 0;
+    const bool ok = comp ? TRTC_Max_Element(V(vec), F(comp), id) : TRTC_Max_Element(V(vec), id);
+    return ok ? (unsigned long long)id : ~0ull;
+}
+TRTC_EXPORT int n_minmax_element(void* vec, void* comp, unsigned long long* ret) {
+    size_t lo = 0, hi = 0;
+    const bool ok = comp ? TRTC_MinMax_Element(V(vec), F(comp), lo, hi) : TRTC_MinMax_Element(V(vec), lo, hi);
+    if (!ok) return -1;
+    ret[0] = lo;
+    ret[1] = hi;
+    return 0;
+}
+TRTC_EXPORT void* n_inner_product(void* vec1, void* vec2, void* init, void* op1, void* op2) {
+    ViewBuf ret;
+    const bool ok = (op1 && op2) ? TRTC_Inner_Product(V(vec1), V(vec2), D(init), ret, F(op1), F(op2))
+                                 : TRTC_Inner_Product(V(vec1), V(vec2), D(init), ret);
+    return ok ? dv_from_viewbuf(ret, D(init).name_view_cls().c_str()) : nullptr;
+}
+#define TRTC_BOOL_EXPORT(name, fn)                        \
+    TRTC_EXPORT int name(void* vec, void* pred) {         \
+        bool r = false;                                   \
+        return fn(V(vec), F(pred), r) ? (r ? 1 : 0) : -1; \
+    }
+TRTC_BOOL_EXPORT(n_all_of, TRTC_All_Of)
+TRTC_BOOL_EXPORT(n_any_of, TRTC_Any_Of)
+TRTC_BOOL_EXPORT(n_none_of, TRTC_None_Of)
+TRTC_BOOL_EXPORT(n_is_partitioned, TRTC_Is_Partitioned)
+#undef TRTC_BOOL_EXPORT
+TRTC_EXPORT int n_is_sorted(void* vec, void* comp) {
+    bool r = false;
+    const bool ok = comp ? TRTC_Is_Sorted(V(vec), F(comp), r) : TRTC_Is_Sorted(V(vec), r);
+    return ok ? (r ? 1 : 0) : -1;
+}
+// searching -- python/api_Searching.cpp: a missing index reads as the size
+static long long index_or_size(bool ok, size_t r, size_t size) {
+    if (!ok) return -1;
+    return r == (size_t)(-1) ? (long long)size : (long long)r;
+}
+TRTC_EXPORT long long n_find(void* vec, void* value) {
+    size_t r = 0;
+    const bool ok = TRTC_Find(V(vec), D(value), r);
+    return index_or_size(ok, r, V(vec).size());
+}
+TRTC_EXPORT long long n_find_if(void* vec, void* pred) {
+    size_t r = 0;
+    const bool ok = TRTC_Find_If(V(vec), F(pred), r);
+    return index_or_size(ok, r, V(vec).size());
+}
+TRTC_EXPORT long long n_find_if_not(void* vec, void* pred) {
+    size_t r = 0;
+    const bool ok = TRTC_Find_If_Not(V(vec), F(pred), r);
+    return index_or_size(ok, r, V(vec).size());
+}
+TRTC_EXPORT long long n_mismatch(void* vec1, void* vec2, void* pred) {
+    size_t r = 0;
+    const bool ok = pred ? TRTC_Mismatch(V(vec1), V(vec2), F(pred), r) : TRTC_Mismatch(V(vec1), V(vec2), r);
+    return index_or_size(ok, r, V(vec1).size());
+}
+TRTC_EXPORT unsigned long long n_partition_point(void* vec, void* pred) {
+    size_t r = 0;
+    if (!TRTC_Partition_Point(V(vec), F(pred), r)) return ~0ull;
+    return r == (size_t)(-1) ? (unsigned long long)V(vec).size() : (unsigned long long)r;
+}
+TRTC_EXPORT unsigned long long n_is_sorted_until(void* vec, void* comp) {
+    size_t r = 0;
+    const bool ok = comp ? TRTC_Is_Sorted_Until(V(vec), F(comp), r) : TRTC_Is_Sorted_Until(V(vec), r);
+    return ok ? (unsigned long long)r : ~0ull;
+}
+// merging -- python/api_Merging.cpp
+TRTC_EXPORT int n_merge(void* vec1, void* vec2, void* out, void* comp) {
+    return (comp ? TRTC_Merge(V(vec1), V(vec2), V(out), F(comp)) : TRTC_Merge(V(vec1), V(vec2), V(out))) ? 0 : -1;
+}
+TRTC_EXPORT int n_merge_by_key(void* k1, void* k2, void* v1, void* v2, void* ko, void* vo, void* comp) {
+    return (comp ? TRTC_Merge_By_Key(V(k1), V(k2), V(v1), V(v2), V(ko), V(vo), F(comp))
+                 : TRTC_Merge_By_Key(V(k1), V(k2), V(v1), V(v2), V(ko), V(vo))) ? 0 : -1;
 }

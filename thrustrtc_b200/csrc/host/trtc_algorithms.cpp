@@ -183,7 +183,7 @@ bool jit_copy(const ViewArg& in, const ViewArg& out, size_t n, size_t in_off = 0
 // Scan-family kernel through NVRTC.  mode: 0 inclusive, 1 exclusive (init), 2 reduce,
 // 3 reduce with init; reductions leave their result in *result_dev.
 bool jit_scan(const DVVectorLike& in, const Functor* uop, const DVVectorLike* out, const std::string& T,
-              const Functor& op, int mode, const ViewBuf& init, void** result_dev) {
+              const Functor& op, int mode, const ViewBuf& init, void** result_dev, const char* extra_header = nullptr) {
     const size_t n = in.size();
     const ViewArg iv = view_arg(in);
     const int vec = iv.contiguous ? vec_width(in.elem_size()) : 1;
@@ -211,7 +211,9 @@ bool jit_scan(const DVVectorLike& in, const Functor* uop, const DVVectorLike* ou
     const std::string k = "trtc::scan_kernel<" + iv.type + ", " + (uop ? uop->name_view_cls() : k_nothing) + ", " +
                           (uop ? "true" : "false") + ", " + ov.type + ", " + T + ", " + op.name_view_cls() + ", " +
                           num(mode) + ", 256, " + num(nv) + ">";
-    const bool ok = jit_run({"trtc_scan.cuh"}, k, (unsigned)tiles, 256,
+    std::vector<std::string> headers{"trtc_scan.cuh"};
+    if (extra_header) headers.push_back(extra_header);
+    const bool ok = jit_run(headers, k, (unsigned)tiles, 256,
                             {iv.bytes, uop ? uop->view() : nothing_bytes(), ov.bytes, pod_bytes<size_t>(n), op.view(),
                              init.size() == tl.size ? init : zero_of(T), st});
     if (result_dev) *result_dev = res;
@@ -875,4 +877,485 @@ bool TRTC_Binary_Search_V(const DVVectorLike& vec, const DVVectorLike& values, D
 }
 bool TRTC_Binary_Search_V(const DVVectorLike& vec, const DVVectorLike& values, DVVectorLike& result) {
     return search_vector(2, vec, values, result, Functor("Less"));
+}
+
+// ====================================================================== remaining algorithms
+// fill.h, sequence.h, tabulate.h, transform.h, replace.h, for_each.h, adjacent_difference.h,
+// gather.h, scatter.h, swap.h, count.h, find.h, mismatch.h, equal.h, logical.h, extrema.h,
+// inner_product.h, partition.h (point, is_partitioned), sort.h (is_sorted*), merge.h: one
+// NVRTC-instantiated kernel of trtc_misc.cuh each, over any views and user functors.
+namespace {
+
+ViewArg nothing_arg() {
+    ViewArg a;
+    a.type = k_nothing;
+    a.bytes = nothing_bytes();
+    return a;
+}
+ViewArg functor_arg(const Functor& f) {
+    ViewArg a;
+    a.type = f.name_view_cls();
+    a.bytes = f.view();
+    return a;
+}
+// a DeviceViewable (scalar, tuple, ...) as a kernel argument of its own view type
+ViewArg dv_arg(const DeviceViewable& d) {
+    ViewArg a;
+    a.type = d.name_view_cls();
+    a.bytes = d.view();
+    return a;
+}
+
+std::string targs(const std::vector<std::string>& parts) {
+    std::string s = "<";
+    for (size_t i = 0; i < parts.size(); i++) s += parts[i] + (i + 1 < parts.size() ? ", " : "");
+    return s + ">";
+}
+
+// one grid-stride launch of trtc::<kernel> over n items; params in the kernel's order
+bool misc_run(const std::string& kernel, const std::vector<ViewArg>& args, size_t n, std::vector<ViewBuf> tail) {
+    if (n == 0) return true;
+    if (!ensure_device()) return false;
+    std::vector<std::string> types;
+    std::vector<ViewBuf> params;
+    for (const ViewArg& a : args) {
+        types.push_back(a.type);
+        params.push_back(a.bytes);
+    }
+    for (auto& t : tail) params.push_back(t);
+    return jit_run({"trtc_misc.cuh"}, "trtc::" + kernel + targs(types), grid_for(n, 256), 256, params);
+}
+// same, with leading non-type template arguments
+bool misc_run_t(const std::string& kernel, const std::vector<std::string>& lead, const std::vector<ViewArg>& args,
+                size_t n, std::vector<ViewBuf> tail) {
+    if (n == 0) return true;
+    if (!ensure_device()) return false;
+    std::vector<std::string> types = lead;
+    std::vector<ViewBuf> params;
+    for (const ViewArg& a : args) {
+        types.push_back(a.type);
+        params.push_back(a.bytes);
+    }
+    for (auto& t : tail) params.push_back(t);
+    return jit_run({"trtc_misc.cuh"}, "trtc::" + kernel + targs(types), grid_for(n, 256), 256, params);
+}
+
+// the value as the vector's element type when it converts on the host, else as itself
+ViewArg value_as_elem(const DeviceViewable& value, const DVVectorLike& vec) {
+    ViewArg a;
+    a.type = vec.name_elem_cls();
+    if (!convert_scalar(value, a.type, a.bytes)) a = dv_arg(value);
+    return a;
+}
+
+// first index in [begin, n) with the property of `mode` (FindMode of trtc_misc.cuh); n if none
+bool find_first(int mode, const ViewArg& v, const ViewArg& w, const ViewArg& value, const ViewArg& pred, size_t begin,
+                size_t n, size_t& result) {
+    result = n;
+    if (begin >= n) return true;
+    if (!ensure_device()) return false;
+    unsigned long long* d = (unsigned long long*)tmp_alloc(8, S());
+    if (!d) return false;
+    const unsigned long long init = n;
+    bool ok = TRTC_CUDA(cudaMemcpyAsync(d, &init, 8, cudaMemcpyHostToDevice, S()));
+    const std::string k = "trtc::find_first_kernel" + targs({num(mode), v.type, w.type, value.type, pred.type});
+    ok = ok && jit_run({"trtc_misc.cuh"}, k, grid_for(n - begin, 256), 256,
+                       {v.bytes, w.bytes, value.bytes, pred.bytes, pod_bytes<size_t>(begin), pod_bytes<size_t>(n),
+                        pod_bytes<unsigned long long*>(d)});
+    unsigned long long r = n;
+    ok = ok && TRTC_CUDA(cudaMemcpyAsync(&r, d, 8, cudaMemcpyDeviceToHost, S())) && check_device_errors(S(), "find");
+    tmp_free(d, S());
+    result = (size_t)r;
+    return ok;
+}
+// general_find's convention (internal/general_find.cpp): (size_t)-1 when nothing is found
+bool find_or_none(int mode, const ViewArg& v, const ViewArg& w, const ViewArg& value, const ViewArg& pred, size_t n,
+                  size_t& result) {
+    size_t r = 0;
+    if (!find_first(mode, v, w, value, pred, 0, n, r)) return false;
+    result = r >= n ? (size_t)(-1) : r;
+    return true;
+}
+
+bool count_run(int mode, const DVVectorLike& vec, const ViewArg& value, const ViewArg& pred, size_t& result) {
+    result = 0;
+    const size_t n = vec.size();
+    if (n == 0) return true;
+    if (!ensure_device()) return false;
+    unsigned long long* d = (unsigned long long*)tmp_alloc(8, S());
+    if (!d) return false;
+    bool ok = TRTC_CUDA(cudaMemsetAsync(d, 0, 8, S()));
+    const ViewArg v = view_arg(vec);
+    ok = ok && jit_run({"trtc_misc.cuh"}, "trtc::count_kernel" + targs({num(mode), v.type, value.type, pred.type}),
+                       grid_for(n, 256), 256,
+                       {v.bytes, value.bytes, pred.bytes, pod_bytes<size_t>(n), pod_bytes<unsigned long long*>(d)});
+    unsigned long long r = 0;
+    ok = ok && TRTC_CUDA(cudaMemcpyAsync(&r, d, 8, cudaMemcpyDeviceToHost, S())) && check_device_errors(S(), "count");
+    tmp_free(d, S());
+    result = (size_t)r;
+    return ok;
+}
+
+// the reference's element-index reduction (MAX, or min, under comp); empty leaves result as is
+bool index_tree(bool max, const DVVectorLike& vec, const Functor& comp, size_t& result) {
+    const size_t n = vec.size();
+    if (n == 0) return true;  // extrema.cpp:8
+    if (!ensure_device()) return false;
+    const ViewArg v = view_arg(vec);
+    const size_t nb1 = (n + 255) / 256;
+    unsigned long long* t[2] = {(unsigned long long*)tmp_alloc(nb1 * 8, S()),
+                                (unsigned long long*)tmp_alloc(nb1 * 8, S())};
+    bool ok = t[0] && t[1];
+    size_t m = n;
+    int cur = 0;  // buffer holding the latest round's results
+    for (bool first = true; ok && (first || m > 1); first = false) {
+        const size_t nb = (m + 255) / 256;
+        const size_t cap = (size_t)sm_count() * 8;
+        const unsigned grid = (unsigned)(nb < cap ? nb : cap);
+        const int dst = first ? 0 : cur ^ 1;
+        const std::string k = "trtc::index_tree_kernel" +
+                              targs({max ? "true" : "false", first ? "true" : "false", v.type, comp.name_view_cls()});
+        ok = jit_run({"trtc_misc.cuh"}, k, grid, 256,
+                     {v.bytes, comp.view(), pod_bytes<const unsigned long long*>(first ? nullptr : t[cur]),
+                      pod_bytes<size_t>(m), pod_bytes<unsigned long long*>(t[dst])});
+        cur = dst;
+        m = nb;
+    }
+    unsigned long long r = 0;
+    ok = ok && TRTC_CUDA(cudaMemcpyAsync(&r, t[cur], 8, cudaMemcpyDeviceToHost, S())) &&
+         check_device_errors(S(), "extrema");
+    if (t[0]) tmp_free(t[0], S());
+    if (t[1]) tmp_free(t[1], S());
+    if (ok) result = (size_t)r;
+    return ok;
+}
+
+// does [p, p + n*es) overlap [q, q + m*es2)?
+bool overlaps(const void* p, size_t bytes_p, const void* q, size_t bytes_q) {
+    const char* a = (const char*)p;
+    const char* b = (const char*)q;
+    return a < b + bytes_q && b < a + bytes_p;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- transformations
+bool TRTC_Fill(DVVectorLike& vec, const DeviceViewable& value) {
+    return misc_run("fill_kernel", {view_arg(vec), dv_arg(value)}, vec.size(), {pod_bytes<size_t>(vec.size())});
+}
+bool TRTC_Sequence(DVVectorLike& vec, const DeviceViewable& value_init, const DeviceViewable& value_step) {
+    return misc_run("sequence_kernel", {view_arg(vec), dv_arg(value_init), dv_arg(value_step)}, vec.size(),
+                    {pod_bytes<size_t>(vec.size())});
+}
+bool TRTC_Sequence(DVVectorLike& vec, const DeviceViewable& value_init) {
+    return TRTC_Sequence(vec, value_init, DVInt32(1));
+}
+bool TRTC_Sequence(DVVectorLike& vec) { return TRTC_Sequence(vec, DVInt32(0), DVInt32(1)); }
+bool TRTC_Tabulate(DVVectorLike& vec, const Functor& op) {
+    return misc_run("tabulate_kernel", {view_arg(vec), functor_arg(op)}, vec.size(), {pod_bytes<size_t>(vec.size())});
+}
+bool TRTC_For_Each(DVVectorLike& vec, const Functor& f) {
+    return misc_run("for_each_kernel", {view_arg(vec), functor_arg(f)}, vec.size(), {pod_bytes<size_t>(vec.size())});
+}
+static bool transform_any(int mode, const DVVectorLike& in, const DVVectorLike* st, DVVectorLike& out,
+                          const Functor& op, const Functor* pred) {
+    return misc_run_t("transform_kernel", {num(mode)},
+                      {view_arg(in), st ? view_arg(*st) : nothing_arg(), view_arg(out), functor_arg(op),
+                       pred ? functor_arg(*pred) : nothing_arg()},
+                      in.size(), {pod_bytes<size_t>(in.size())});
+}
+bool TRTC_Transform(const DVVectorLike& in, DVVectorLike& out, const Functor& op) {
+    return transform_any(0, in, nullptr, out, op, nullptr);
+}
+bool TRTC_Transform_If(const DVVectorLike& in, DVVectorLike& out, const Functor& op, const Functor& pred) {
+    return transform_any(1, in, nullptr, out, op, &pred);
+}
+bool TRTC_Transform_If_Stencil(const DVVectorLike& in, const DVVectorLike& stencil, DVVectorLike& out,
+                               const Functor& op, const Functor& pred) {
+    return transform_any(2, in, &stencil, out, op, &pred);
+}
+static bool transform_binary_any(bool stencil, const DVVectorLike& in1, const DVVectorLike& in2,
+                                 const DVVectorLike* st, DVVectorLike& out, const Functor& op, const Functor* pred) {
+    return misc_run_t("transform_binary_kernel", {stencil ? "true" : "false"},
+                      {view_arg(in1), view_arg(in2), st ? view_arg(*st) : nothing_arg(), view_arg(out),
+                       functor_arg(op), pred ? functor_arg(*pred) : nothing_arg()},
+                      in1.size(), {pod_bytes<size_t>(in1.size())});
+}
+bool TRTC_Transform_Binary(const DVVectorLike& in1, const DVVectorLike& in2, DVVectorLike& out, const Functor& op) {
+    return transform_binary_any(false, in1, in2, nullptr, out, op, nullptr);
+}
+bool TRTC_Transform_Binary_If_Stencil(const DVVectorLike& in1, const DVVectorLike& in2, const DVVectorLike& stencil,
+                                      DVVectorLike& out, const Functor& op, const Functor& pred) {
+    return transform_binary_any(true, in1, in2, &stencil, out, op, &pred);
+}
+// replace.cpp: both values are converted to the input's element type before use
+static bool replace_any(bool use_pred, const DVVectorLike& in, DVVectorLike& out, const DeviceViewable* old_value,
+                        const Functor* pred, const DeviceViewable& new_value) {
+    const ViewArg nv = value_as_elem(new_value, in);
+    const ViewArg ov = old_value ? value_as_elem(*old_value, in) : nv;
+    if (ov.type != nv.type) {
+        set_error("replace: old and new values must convert to the element type");
+        return false;
+    }
+    return misc_run_t("replace_kernel", {use_pred ? "true" : "false"},
+                      {view_arg(in), view_arg(out), ov, pred ? functor_arg(*pred) : nothing_arg(), nv}, in.size(),
+                      {pod_bytes<size_t>(in.size())});
+}
+bool TRTC_Replace(DVVectorLike& vec, const DeviceViewable& old_value, const DeviceViewable& new_value) {
+    return replace_any(false, vec, vec, &old_value, nullptr, new_value);
+}
+bool TRTC_Replace_If(DVVectorLike& vec, const Functor& pred, const DeviceViewable& new_value) {
+    return replace_any(true, vec, vec, nullptr, &pred, new_value);
+}
+bool TRTC_Replace_Copy(const DVVectorLike& in, DVVectorLike& out, const DeviceViewable& old_value,
+                       const DeviceViewable& new_value) {
+    return replace_any(false, in, out, &old_value, nullptr, new_value);
+}
+bool TRTC_Replace_Copy_If(const DVVectorLike& in, DVVectorLike& out, const Functor& pred,
+                          const DeviceViewable& new_value) {
+    return replace_any(true, in, out, nullptr, &pred, new_value);
+}
+// out[0] = in[0], out[i] = op(in[i], in[i-1]) (adjacent_difference.cpp:3-25).  An output that
+// may share memory with the input reads from a copy of it, so in-place calls are well defined.
+bool TRTC_Adjacent_Difference(const DVVectorLike& in, DVVectorLike& out, const Functor& op) {
+    const size_t n = in.size();
+    if (n == 0) return true;
+    if (!ensure_device()) return false;
+    std::unique_ptr<DVVector> tmp;
+    const DVVectorLike* src = &in;
+    const void* ip = in.contiguous_data();
+    const void* opp = out.contiguous_data();
+    if (!ip || !opp || overlaps(ip, n * in.elem_size(), opp, out.size() * out.elem_size())) {
+        tmp.reset(new DVVector(in.name_elem_cls().c_str(), n));
+        if (!jit_copy(view_arg(in), view_arg(*tmp), n)) return false;
+        src = tmp.get();
+    }
+    return misc_run("adjacent_difference_kernel", {view_arg(*src), view_arg(out), functor_arg(op)}, n,
+                    {pod_bytes<size_t>(n)});
+}
+bool TRTC_Adjacent_Difference(const DVVectorLike& in, DVVectorLike& out) {
+    return TRTC_Adjacent_Difference(in, out, Functor("Minus"));
+}
+
+// ---------------------------------------------------------------- copying
+static bool gather_any(int sel, const DVVectorLike& map, const DVVectorLike* st, const DVVectorLike& in,
+                       DVVectorLike& out, const Functor* pred) {
+    return misc_run_t("gather_kernel", {num(sel)},
+                      {view_arg(map), st ? view_arg(*st) : nothing_arg(), view_arg(in), view_arg(out),
+                       pred ? functor_arg(*pred) : nothing_arg()},
+                      map.size(), {pod_bytes<size_t>(map.size())});
+}
+bool TRTC_Gather(const DVVectorLike& map, const DVVectorLike& in, DVVectorLike& out) {
+    return gather_any(0, map, nullptr, in, out, nullptr);
+}
+bool TRTC_Gather_If(const DVVectorLike& map, const DVVectorLike& stencil, const DVVectorLike& in, DVVectorLike& out) {
+    return gather_any(1, map, &stencil, in, out, nullptr);
+}
+bool TRTC_Gather_If(const DVVectorLike& map, const DVVectorLike& stencil, const DVVectorLike& in, DVVectorLike& out,
+                    const Functor& pred) {
+    return gather_any(2, map, &stencil, in, out, &pred);
+}
+static bool scatter_any(int sel, const DVVectorLike& in, const DVVectorLike& map, const DVVectorLike* st,
+                        DVVectorLike& out, const Functor* pred) {
+    return misc_run_t("scatter_kernel", {num(sel)},
+                      {view_arg(in), view_arg(map), st ? view_arg(*st) : nothing_arg(), view_arg(out),
+                       pred ? functor_arg(*pred) : nothing_arg()},
+                      in.size(), {pod_bytes<size_t>(in.size())});
+}
+bool TRTC_Scatter(const DVVectorLike& in, const DVVectorLike& map, DVVectorLike& out) {
+    return scatter_any(0, in, map, nullptr, out, nullptr);
+}
+bool TRTC_Scatter_If(const DVVectorLike& in, const DVVectorLike& map, const DVVectorLike& stencil,
+                     DVVectorLike& out) {
+    return scatter_any(1, in, map, &stencil, out, nullptr);
+}
+bool TRTC_Scatter_If(const DVVectorLike& in, const DVVectorLike& map, const DVVectorLike& stencil,
+                     DVVectorLike& out, const Functor& pred) {
+    return scatter_any(2, in, map, &stencil, out, &pred);
+}
+bool TRTC_Swap(DVVectorLike& a, DVVectorLike& b) {
+    return misc_run("swap_kernel", {view_arg(a), view_arg(b)}, a.size(), {pod_bytes<size_t>(a.size())});
+}
+
+// ---------------------------------------------------------------- reductions
+// count.cpp: the value is converted to the element type (vec[i] == (value_t)value)
+bool TRTC_Count(const DVVectorLike& vec, const DeviceViewable& value, size_t& result) {
+    return count_run(0, vec, value_as_elem(value, vec), nothing_arg(), result);
+}
+bool TRTC_Count_If(const DVVectorLike& vec, const Functor& pred, size_t& result) {
+    return count_run(1, vec, nothing_arg(), functor_arg(pred), result);
+}
+bool TRTC_Equal(const DVVectorLike& vec1, const DVVectorLike& vec2, bool& result) {
+    size_t r = 0;
+    if (!find_first(5, view_arg(vec1), view_arg(vec2), nothing_arg(), nothing_arg(), 0, vec1.size(), r)) return false;
+    result = r >= vec1.size();
+    return true;
+}
+bool TRTC_Equal(const DVVectorLike& vec1, const DVVectorLike& vec2, const Functor& pred, bool& result) {
+    size_t r = 0;
+    if (!find_first(3, view_arg(vec1), view_arg(vec2), nothing_arg(), functor_arg(pred), 0, vec1.size(), r))
+        return false;
+    result = r >= vec1.size();
+    return true;
+}
+// logical.cpp: an empty range gives all_of false, any_of false, none_of true
+bool TRTC_All_Of(const DVVectorLike& vec, const Functor& pred, bool& result) {
+    result = false;
+    if (vec.size() < 1) return true;
+    size_t r = 0;
+    if (!find_first(2, view_arg(vec), nothing_arg(), nothing_arg(), functor_arg(pred), 0, vec.size(), r))
+        return false;
+    result = r >= vec.size();
+    return true;
+}
+bool TRTC_Any_Of(const DVVectorLike& vec, const Functor& pred, bool& result) {
+    result = false;
+    if (vec.size() < 1) return true;
+    size_t r = 0;
+    if (!find_first(1, view_arg(vec), nothing_arg(), nothing_arg(), functor_arg(pred), 0, vec.size(), r))
+        return false;
+    result = r < vec.size();
+    return true;
+}
+bool TRTC_None_Of(const DVVectorLike& vec, const Functor& pred, bool& result) {
+    result = true;
+    if (vec.size() < 1) return true;
+    bool any = false;
+    if (!TRTC_Any_Of(vec, pred, any)) return false;
+    result = !any;
+    return true;
+}
+bool TRTC_Min_Element(const DVVectorLike& vec, const Functor& comp, size_t& id_min) {
+    return index_tree(false, vec, comp, id_min);
+}
+bool TRTC_Max_Element(const DVVectorLike& vec, const Functor& comp, size_t& id_max) {
+    return index_tree(true, vec, comp, id_max);
+}
+bool TRTC_Max_Element(const DVVectorLike& vec, size_t& id_max) { return index_tree(true, vec, Functor("Less"), id_max); }
+// both indices of the reference's Pair reduction: the same tree shape for each half
+bool TRTC_MinMax_Element(const DVVectorLike& vec, const Functor& comp, size_t& id_min, size_t& id_max) {
+    return index_tree(false, vec, comp, id_min) && index_tree(true, vec, comp, id_max);
+}
+bool TRTC_MinMax_Element(const DVVectorLike& vec, size_t& id_min, size_t& id_max) {
+    return TRTC_MinMax_Element(vec, Functor("Less"), id_min, id_max);
+}
+
+namespace {
+// BinaryTransformView<T, A, B, Op> { A _a; B _b; Op _op; }: element i = op(a[i], b[i]) in T
+class DVBinaryTransform : public DVVectorLike {
+public:
+    DVBinaryTransform(const std::string& T, const DVVectorLike& a, const DVVectorLike& b, const Functor& op)
+        : DVVectorLike(T.c_str(), T.c_str(), a.size()) {
+        const ViewArg x = view_arg(a), y = view_arg(b);
+        m_name_view_cls = "trtc::BinaryTransformView<" + T + ", " + x.type + ", " + y.type + ", " +
+                          op.name_view_cls() + ">";
+        StructLayout sl;
+        const Layout lx = x.contiguous ? Layout{16, 8} : Layout{a.view_size(), a.view_align()};
+        const Layout ly = y.contiguous ? Layout{16, 8} : Layout{b.view_size(), b.view_align()};
+        const size_t o0 = sl.add(lx), o1 = sl.add(ly), o2 = sl.add(Layout{op.view_size(), op.view_align()});
+        const Layout l = sl.finish();
+        m_buf.assign(l.size, 0);
+        const ViewBuf fv = op.view();
+        memcpy(m_buf.data() + o0, x.bytes.data(), x.bytes.size());
+        memcpy(m_buf.data() + o1, y.bytes.data(), y.bytes.size());
+        memcpy(m_buf.data() + o2, fv.data(), fv.size());
+        m_view_size = l.size;
+        m_view_align = l.align;
+        layout_register(m_name_view_cls, l);
+    }
+    ViewBuf view() const override { return m_buf; }
+
+private:
+    ViewBuf m_buf;
+};
+}  // namespace
+
+// init op1 op2(a0, b0) op1 op2(a1, b1) ... in the init's type (inner_product.cpp:4-30)
+bool TRTC_Inner_Product(const DVVectorLike& vec1, const DVVectorLike& vec2, const DeviceViewable& init, ViewBuf& ret,
+                        const Functor& op1, const Functor& op2) {
+    const std::string T = init.name_view_cls();
+    if (vec1.size() == 0) { ret = init.view(); return true; }
+    if (!ensure_device()) return false;
+    Layout tl;
+    if (!layout_of(T, tl)) { set_error("inner_product: unknown value type " + T); return false; }
+    DVBinaryTransform terms(T, vec1, vec2, op2);
+    void* res = nullptr;
+    if (!jit_scan(terms, nullptr, nullptr, T, op1, 3, init.view(), &res, "trtc_misc.cuh")) return false;
+    return fetch_result(res, tl.size, ret, tl.size > 16);
+}
+bool TRTC_Inner_Product(const DVVectorLike& vec1, const DVVectorLike& vec2, const DeviceViewable& init,
+                        ViewBuf& ret) {
+    return TRTC_Inner_Product(vec1, vec2, init, ret, Functor("Plus"), Functor("trtc::ProductOf"));
+}
+
+// ---------------------------------------------------------------- searching
+// find.cpp / mismatch.cpp: (size_t)-1 when there is no such index
+bool TRTC_Find(const DVVectorLike& vec, const DeviceViewable& value, size_t& result) {
+    return find_or_none(0, view_arg(vec), nothing_arg(), dv_arg(value), nothing_arg(), vec.size(), result);
+}
+bool TRTC_Find_If(const DVVectorLike& vec, const Functor& pred, size_t& result) {
+    return find_or_none(1, view_arg(vec), nothing_arg(), nothing_arg(), functor_arg(pred), vec.size(), result);
+}
+bool TRTC_Find_If_Not(const DVVectorLike& vec, const Functor& pred, size_t& result) {
+    return find_or_none(2, view_arg(vec), nothing_arg(), nothing_arg(), functor_arg(pred), vec.size(), result);
+}
+bool TRTC_Mismatch(const DVVectorLike& vec1, const DVVectorLike& vec2, size_t& result) {
+    return find_or_none(4, view_arg(vec1), view_arg(vec2), nothing_arg(), nothing_arg(), vec1.size(), result);
+}
+bool TRTC_Mismatch(const DVVectorLike& vec1, const DVVectorLike& vec2, const Functor& pred, size_t& result) {
+    return find_or_none(3, view_arg(vec1), view_arg(vec2), nothing_arg(), functor_arg(pred), vec1.size(), result);
+}
+// sort.cpp:93-103: first i with comp(v[i], v[i-1]), else the size
+bool TRTC_Is_Sorted_Until(const DVVectorLike& vec, const Functor& comp, size_t& result) {
+    return find_first(6, view_arg(vec), nothing_arg(), nothing_arg(), functor_arg(comp), 1, vec.size(), result);
+}
+bool TRTC_Is_Sorted_Until(const DVVectorLike& vec, size_t& result) {
+    return TRTC_Is_Sorted_Until(vec, Functor("Less"), result);
+}
+bool TRTC_Is_Sorted(const DVVectorLike& vec, const Functor& comp, bool& result) {
+    size_t r = 0;
+    if (!TRTC_Is_Sorted_Until(vec, comp, r)) return false;
+    result = r >= vec.size();
+    return true;
+}
+bool TRTC_Is_Sorted(const DVVectorLike& vec, bool& result) { return TRTC_Is_Sorted(vec, Functor("Less"), result); }
+// partition.cpp:127-197: fails on an empty range; for a partitioned range the first index
+// whose element fails pred (the size when all pass)
+bool TRTC_Partition_Point(const DVVectorLike& vec, const Functor& pred, size_t& result) {
+    if (vec.size() == 0) return false;
+    return find_first(2, view_arg(vec), nothing_arg(), nothing_arg(), functor_arg(pred), 0, vec.size(), result);
+}
+// partition.cpp:199-214: no element satisfying pred right after one that does not
+bool TRTC_Is_Partitioned(const DVVectorLike& vec, const Functor& pred, bool& result) {
+    result = true;
+    if (vec.size() == 0) return true;
+    size_t r = 0;
+    if (!find_first(7, view_arg(vec), nothing_arg(), nothing_arg(), functor_arg(pred), 1, vec.size(), r)) return false;
+    result = r >= vec.size();
+    return true;
+}
+
+// ---------------------------------------------------------------- merging
+bool TRTC_Merge(const DVVectorLike& a, const DVVectorLike& b, DVVectorLike& out, const Functor& comp) {
+    const size_t n = a.size() > b.size() ? a.size() : b.size();
+    return misc_run_t("merge_kernel", {"false"},
+                      {view_arg(a), view_arg(b), view_arg(out), nothing_arg(), nothing_arg(), nothing_arg(),
+                       functor_arg(comp)},
+                      n, {pod_bytes<size_t>(a.size()), pod_bytes<size_t>(b.size())});
+}
+bool TRTC_Merge(const DVVectorLike& a, const DVVectorLike& b, DVVectorLike& out) {
+    return TRTC_Merge(a, b, out, Functor("Less"));
+}
+bool TRTC_Merge_By_Key(const DVVectorLike& keys1, const DVVectorLike& keys2, const DVVectorLike& values1,
+                       const DVVectorLike& values2, DVVectorLike& keys_out, DVVectorLike& values_out,
+                       const Functor& comp) {
+    const size_t n = keys1.size() > keys2.size() ? keys1.size() : keys2.size();
+    return misc_run_t("merge_kernel", {"true"},
+                      {view_arg(keys1), view_arg(keys2), view_arg(keys_out), view_arg(values1), view_arg(values2),
+                       view_arg(values_out), functor_arg(comp)},
+                      n, {pod_bytes<size_t>(keys1.size()), pod_bytes<size_t>(keys2.size())});
+}
+bool TRTC_Merge_By_Key(const DVVectorLike& keys1, const DVVectorLike& keys2, const DVVectorLike& values1,
+                       const DVVectorLike& values2, DVVectorLike& keys_out, DVVectorLike& values_out) {
+    return TRTC_Merge_By_Key(keys1, keys2, values1, values2, keys_out, values_out, Functor("Less"));
 }
