@@ -268,6 +268,15 @@ __global__ void __launch_bounds__(BLOCK) radix_count_below_kernel(const typename
 }
 
 // ------------------------------------------------------------------ one digit pass
+// 4- or 8-byte asynchronous copy global -> shared (cp.async, L1-allocating)
+template <class V>
+TRTC_FORCEINLINE void cp_async_elem(V* smem_dst, const V* gsrc) {
+    static_assert(sizeof(V) == 4 || sizeof(V) == 8, "cp.async element of 4 or 8 bytes");
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gsrc), "n"((int)sizeof(V)) : "memory");
+}
+TRTC_FORCEINLINE void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Digit of byte `pass` of the ordered key code: one byte permute on the 32-bit half that
 // holds it (sel = 0x4440 | byte index within the half).
 template <class K, bool DESC>
@@ -283,20 +292,55 @@ TRTC_FORCEINLINE uint32_t radix_digit_sel(typename RadixKey<K>::B k, uint32_t se
 template <bool B> struct BoolC { static constexpr bool value = B; };
 
 #ifndef TRTC_RADIX_MINB  // resident CTAs per SM the pass kernel is compiled for
-#define TRTC_RADIX_MINB(items) ((items) >= 24 ? 2 : 3)
+#define TRTC_RADIX_MINB(items) ((items) >= 24 ? 2 : 4)
 #endif
 #ifndef TRTC_RADIX_LB
 #define TRTC_RADIX_LB 4  // predecessor tiles polled per look-back round
 #endif
+// Peer groups of equal digit inside a warp come from two methods that load different
+// pipes: items i with i % MIXP < MIXB use eight bit ballots (ALU and vote instructions),
+// the others atomicOr their lane bit into a per-warp mask per digit in shared memory (LSU).
+// Measured on B200 (2^28 u32 pairs): masks alone move the pass onto the LSU pipe, ballots
+// alone onto issue; one item in three on ballots balances them.  __match_any_sync was 50 %
+// slower than either.
+#ifndef TRTC_RADIX_MIXP
+#define TRTC_RADIX_MIXP 3
+#endif
+#ifndef TRTC_RADIX_MIXB
+#define TRTC_RADIX_MIXB 1
+#endif
+// ranks of item i are resolved (shuffle from the group leader) RWIN items after its atomic:
+// the window covers the atomic's latency and bounds the live per-item state (resolving all
+// ranks after the loop spilled)
+#ifndef TRTC_RADIX_RWIN
+#define TRTC_RADIX_RWIN 4
+#endif
+// payloads copied global -> staging slot with cp.async after the block scan (no registers
+// held across the ranking, which makes room for 4 CTAs per SM) instead of loaded into
+// registers before it
+#ifndef TRTC_RADIX_VASYNC
+#define TRTC_RADIX_VASYNC 1
+#endif
+// the digit masks: two alternating sets of 256 words per warp, placed in the key/payload
+// staging area (idle during the ranking) when it is large enough, else after the counters
+template <int BLOCK>
+constexpr size_t radix_match_words() { return (size_t)(BLOCK / 32) * 2 * 256; }
+template <class KB, class V, bool HAS_VALS, int BLOCK, int TILE>
+constexpr size_t radix_match_smem() {
+    return (TRTC_RADIX_MIXB < TRTC_RADIX_MIXP &&
+            (size_t)TILE * (sizeof(KB) + (HAS_VALS ? sizeof(V) : 0)) < radix_match_words<BLOCK>() * 4)
+               ? radix_match_words<BLOCK>() * 4 : (size_t)0;
+}
 
 // HAS_VALS: move a 4- or 8-byte payload with the keys.  vals_from_index: the payload of the
 // first active pass is the element index (used to sort a permutation for odd value sizes).
 //
 // Per tile (BLOCK threads x ITEMS keys, warp-striped: key i of lane l of warp w sits at
 // tile_base + w*32*ITEMS + i*32 + l):
-//   1. load the keys; rank every key inside its warp (peers of equal digit from 8 bit
-//      ballots, one shared-memory atomicAdd per peer group on the warp's digit counters);
-//   2. issue the payload loads (they complete while the counts are scanned);
+//   1. load the keys; rank every key inside its warp (peers of equal digit from bit
+//      ballots or shared-memory digit masks, one shared-memory atomicAdd per peer group on
+//      the warp's digit counters);
+//   2. (payloads are not held in registers: step 4 copies them with cp.async)
 //   3. one thread per digit: tile count, publication of the tile aggregate, block-wide
 //      exclusive scan of the counts, warp offsets folded into the warp counters;
 //   4. stage keys (and payloads) in shared memory in digit order; then, one thread per
@@ -322,6 +366,9 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
     KB* s_keys = reinterpret_cast<KB*>(smem);
     V* s_vals = reinterpret_cast<V*>(smem + sizeof(KB) * TILE);
     uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem + sizeof(KB) * TILE + (HAS_VALS ? sizeof(V) * TILE : 0));
+    // digit masks (see radix_match_smem)
+    uint32_t* s_wmatch = radix_match_smem<KB, V, HAS_VALS, BLOCK, TILE>() ? s_whist + WARPS * 256
+                                                                         : reinterpret_cast<uint32_t*>(smem);
     __shared__ IX s_adj[256];
     __shared__ uint32_t s_wsum[8];
     __shared__ uint32_t s_tile;
@@ -349,6 +396,8 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
 
     if (threadIdx.x == 0) s_tile = atomicAdd(&ctrl->tile_ctr[ord], 1u);
     for (int i = threadIdx.x; i < WARPS * 256; i += BLOCK) s_whist[i] = 0;
+    if (TRTC_RADIX_MIXB < TRTC_RADIX_MIXP)
+        for (int i = threadIdx.x; i < (int)radix_match_words<BLOCK>(); i += BLOCK) s_wmatch[i] = 0;
     __syncthreads();
     const size_t tile = s_tile;
     st_next[tile * 256 + threadIdx.x] = 0;
@@ -378,15 +427,32 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
         }
         const uint32_t ltm = lanemask_lt();
         uint32_t info[ITEMS];  // rank among peers | group leader lane << 8
+        constexpr int RW = (TRTC_RADIX_RWIN > 0 && TRTC_RADIX_RWIN < ITEMS) ? TRTC_RADIX_RWIN : ITEMS;
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t d = radix_digit_sel<K, DESC>(keys[i], sel, hi);
-            uint32_t peers = FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, (uint32_t)i * 32u + lane < warp_n);
+            uint32_t peers;
+            if ((i % TRTC_RADIX_MIXP) < TRTC_RADIX_MIXB) {
+                peers = FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, (uint32_t)i * 32u + lane < warp_n);
 #pragma unroll
-            for (int b = 0; b < 8; b++) {
-                const bool bit = (d >> b) & 1u;
-                const uint32_t bb = __ballot_sync(0xffffffffu, bit);
-                peers &= bit ? bb : ~bb;
+                for (int b = 0; b < 8; b++) {
+                    const bool bit = (d >> b) & 1u;
+                    const uint32_t bb = __ballot_sync(0xffffffffu, bit);
+                    peers &= bit ? bb : ~bb;
+                }
+            } else {
+                const bool valid = FULL || (uint32_t)i * 32u + lane < warp_n;
+                // the two mask sets alternate over the mask-ranked items, so a set is reused
+                // only after the other set's item and its two warp barriers
+                const int ors_before = i - ((i / TRTC_RADIX_MIXP) * TRTC_RADIX_MIXB +
+                                            ((i % TRTC_RADIX_MIXP) < TRTC_RADIX_MIXB ? (i % TRTC_RADIX_MIXP)
+                                                                                     : TRTC_RADIX_MIXB));
+                uint32_t* wm = s_wmatch + warp * 512 + (ors_before & 1) * 256;
+                if (valid) atomicOr(&wm[d], 1u << lane);
+                __syncwarp();
+                peers = valid ? wm[d] : 0u;
+                __syncwarp();
+                if (valid && lane == 31u - __clz(peers)) wm[d] = 0u;
             }
             // the highest lane of a group adds the group's size to the warp's digit counter
             const uint32_t leader = 31u - __clz(peers);
@@ -394,12 +460,16 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
             rank[i] = 0;
             if (lane == leader && (FULL || (uint32_t)i * 32u + lane < warp_n))
                 rank[i] = atomicAdd(&wh[d], (uint32_t)__popc(peers));
+            if (i >= RW) {
+                const int j = i - RW;
+                rank[j] = __shfl_sync(0xffffffffu, rank[j], (int)(info[j] >> 8)) + (info[j] & 0xFFu);
+            }
         }
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++)
-            rank[i] = __shfl_sync(0xffffffffu, rank[i], (int)(info[i] >> 8)) + (info[i] & 0xFFu);
+        for (int j = ITEMS - RW; j < ITEMS; j++)
+            rank[j] = __shfl_sync(0xffffffffu, rank[j], (int)(info[j] >> 8)) + (info[j] & 0xFFu);
         // ---- 2. payload loads, consumed only at staging
-        if constexpr (HAS_VALS) {
+        if constexpr (HAS_VALS && !TRTC_RADIX_VASYNC) {
             const V* __restrict__ wv = src_v + wbase;
 #pragma unroll
             for (int i = 0; i < ITEMS; i++) {
@@ -437,9 +507,18 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
             const uint32_t d = radix_digit_sel<K, DESC>(keys[i], sel, hi);
             const uint32_t pos = wh[d] + rank[i];
             s_keys[pos] = keys[i];
-            if (HAS_VALS) s_vals[pos] = vals[i];
+            if constexpr (HAS_VALS) {
+                if constexpr (TRTC_RADIX_VASYNC) {
+                    const uint32_t r = (uint32_t)i * 32u + lane;
+                    if (index_payload) s_vals[pos] = (V)(wbase + r);
+                    else cp_async_elem(&s_vals[pos], src_v + wbase + r);
+                } else {
+                    s_vals[pos] = vals[i];
+                }
+            }
         }
     }
+    if constexpr (HAS_VALS && TRTC_RADIX_VASYNC) cp_async_wait_all();  // before the barrier below
 
     // ---- decoupled look-back for the digit's global offset.  Each round polls LB
     // predecessor tiles at once (independent loads), so the inclusive-prefix frontier

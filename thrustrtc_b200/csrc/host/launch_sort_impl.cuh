@@ -106,7 +106,8 @@ static bool radix_sort_run(K* keys, V* vals0, size_t n, cudaStream_t s, int vals
             count_launch();
             ktimer_mark("radix_nan_rotation", s);
         }
-        const size_t smem = (size_t)TILE * sizeof(KB) + (HAS_VALS ? (size_t)TILE * sizeof(V) : 0) + (BLOCK / 32) * 256 * 4;
+        const size_t smem = (size_t)TILE * sizeof(KB) + (HAS_VALS ? (size_t)TILE * sizeof(V) : 0) + (BLOCK / 32) * 256 * 4 +
+                            radix_match_smem<KB, V, HAS_VALS, BLOCK, TILE>();
         auto pass_kernel = radix_pass_kernel<K, V, HAS_VALS, DESC, BLOCK, ITEMS, ST>;
         set_smem_attr_once(pass_kernel, smem);
         for (int p = 0; p < D; p++) {
