@@ -1015,7 +1015,7 @@ def _srv_sigs(L):
 
 
 def run_serving(args):
-    """Poisson arrivals of mixed requests into the request server (continuous batching: 4
+    """Poisson arrivals of mixed requests into the request server (continuous batching: 8
     streams, coalescing of requests up to 2^16 elements, 32 GB admission budget) beside the
     plain path (the same requests one call at a time, no coalescing, one stream).  Offered
     load is swept over fractions of each path's closed-loop capacity."""
@@ -1116,7 +1116,7 @@ def run_serving(args):
         return cap, levels
 
     budget = 32 << 30
-    srv = L.trtc_server_create(budget, 4, 1 << 16)
+    srv = L.trtc_server_create(budget, 8, 1 << 16)
     if not srv:
         raise RuntimeError(N.last_error())
     lc0 = N.launch_count()
@@ -1138,7 +1138,7 @@ def run_serving(args):
                        "mix": "60% Sort_By_Key (+uint32 values), 25% exclusive scan, 15% reduce",
                        "sizes": "log-uniform 2^10..2^24", "types": "uint32 / int64 / float equal shares",
                        "elements_per_level": elems, "budget_bytes": budget,
-                       "server": "4 streams, coalescing up to 2^16 elements per request, admission by budget",
+                       "server": "8 streams, coalescing up to 2^16 elements per request, admission by budget",
                        "plain": "same requests, one call at a time on one stream, no coalescing",
                        "load_levels": "fractions of each path's closed-loop capacity"},
             "capacity_rps": {"served": cap_b, "plain": cap_p, "ratio": cap_b / cap_p},

@@ -7,12 +7,16 @@
 
 namespace trtc_host {
 
-// items per thread of a digit pass (tile = 256 * ITEMS keys), from a sweep on B200 at 2^28
-// u32 pairs (16: 7.15 ms, 20: 7.01 ms, 24 with 2 CTAs/SM: 7.12 ms)
+// items per thread of a digit pass (tile = 256 * ITEMS keys), from sweeps on B200: 2^28 u32
+// pairs 6.13 ms at 20 (4 CTAs/SM), 6.16 ms at 24 (3 CTAs/SM); 2^24 i64 keys + u32 values
+// 1.48 ms at 8, 1.33 at 10, 1.18 at 12 (4 CTAs/SM), 1.18 at 16 (3 CTAs/SM, spills)
 #ifndef TRTC_RADIX_ITEMS32
 #define TRTC_RADIX_ITEMS32 20
 #endif
-template <class K> struct SortTuning { enum { ITEMS = sizeof(K) >= 8 ? 8 : TRTC_RADIX_ITEMS32 }; };
+#ifndef TRTC_RADIX_ITEMS64
+#define TRTC_RADIX_ITEMS64 12
+#endif
+template <class K> struct SortTuning { enum { ITEMS = sizeof(K) >= 8 ? TRTC_RADIX_ITEMS64 : TRTC_RADIX_ITEMS32 }; };
 
 // Opts a kernel in to `bytes` of dynamic shared memory (needed as soon as static +
 // dynamic exceeds 48 KB).  Tracked per kernel address: many instantiations share one type.
