@@ -163,6 +163,11 @@ __global__ void __launch_bounds__(BLOCK, 4) compact2_kernel(InV in, StV stencil,
                            !PARTITION && (MODE == CM_PRED || MODE == CM_NOT_EQUAL || MODE == CM_NOT_PRED);
     constexpr int VROWS = ITEMS / 4;
     typedef union { uint4 q; E t[4]; } Vec;
+    // vector path: each warp gathers its selected elements in shared memory (placed so that
+    // 16-byte aligned output addresses map to 16-byte aligned slots), then writes them with
+    // 16-byte stores (scalar stores only at the run's ragged ends)
+    constexpr int WSTAGE = 32 * ITEMS + 4;
+    __shared__ __align__(16) E s_stage[VECOK ? WARPS * WSTAGE : 1];
     auto vec_fast = [&](size_t tile) -> bool {
         if constexpr (VECOK) return (tile + 1) * (size_t)TILE <= n && ((((size_t)in._data) & 15) == 0);
         else return false;
@@ -284,6 +289,10 @@ __global__ void __launch_bounds__(BLOCK, 4) compact2_kernel(InV in, StV stencil,
 #pragma unroll
                 for (int r = 0; r < VROWS; r++) u[r].q = p[r * 32 + lane];
                 const unsigned long long out_n = out.size();
+                E* sbuf = s_stage + warp * WSTAGE;
+                // slot j of sbuf holds output element run + (j - s0)
+                const uint32_t s0 = (uint32_t)((reinterpret_cast<size_t>(out._data + run) >> 2) & 3u);
+                uint32_t tot = 0;
 #pragma unroll
                 for (int r = 0; r < VROWS; r++) {
                     bool f[4];
@@ -296,16 +305,27 @@ __global__ void __launch_bounds__(BLOCK, 4) compact2_kernel(InV in, StV stencil,
                         const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
                         if (lane >= (uint32_t)d) x += y;
                     }
-                    unsigned long long pos = run + (x - c);
+                    uint32_t pos = s0 + tot + (x - c);
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        if (f[e]) {
-                            if (pos < out_n) out._data[pos] = u[r].t[e];
-                            pos++;
+                    for (int e = 0; e < 4; e++)
+                        if (f[e]) sbuf[pos++] = u[r].t[e];
+                    tot += __shfl_sync(0xffffffffu, x, 31);
+                }
+                __syncwarp();
+                const uint32_t end = s0 + tot;
+                for (uint32_t j0 = lane * 4; j0 < end; j0 += 128) {
+                    const unsigned long long g0 = run + j0 - s0;  // output index of slot j0 (j0 >= s0)
+                    if (j0 >= s0 && j0 + 4 <= end && g0 + 4 <= out_n) {
+                        *reinterpret_cast<uint4*>(out._data + g0) = *reinterpret_cast<const uint4*>(sbuf + j0);
+                    } else {
+#pragma unroll
+                        for (uint32_t k = 0; k < 4; k++) {
+                            const uint32_t j = j0 + k;
+                            if (j >= s0 && j < end && run + (j - s0) < out_n) out._data[run + (j - s0)] = sbuf[j];
                         }
                     }
-                    run += __shfl_sync(0xffffffffu, x, 31);
                 }
+                __syncwarp();  // the buffer is refilled by this warp's next tile
             }
         } else {
             E v[ITEMS];

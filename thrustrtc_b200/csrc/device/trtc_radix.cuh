@@ -252,16 +252,40 @@ __global__ void __launch_bounds__(256) min_tree_kernel(const typename RadixKey<K
     }
 }
 
-// number of keys whose ordered code is below the selected minimum's (NaN case only)
+// number of keys whose ordered code is below the selected minimum's (NaN case only).
+// 16-byte loads, four per thread in flight (a scalar grid-stride loop kept too few bytes in
+// flight to reach HBM bandwidth); ragged head and tail elements are read one by one.
 template <class K, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) radix_count_below_kernel(const typename RadixKey<K>::B* __restrict__ keys, size_t n,
                                                                   const unsigned long long* min_idx, SortCtrl* ctrl) {
     if (ctrl->nan_flag == 0) return;
     typedef RadixKey<K> RK;
+    typedef typename RK::B KB;
+    constexpr int PER = 16 / sizeof(KB);
     const typename RK::U tm = RK::ordered(keys[*min_idx]);
+    const size_t mis = ((16u - ((size_t)keys & 15u)) & 15u) / sizeof(KB);
+    const size_t head = mis < n ? mis : n;
+    const size_t nvec = (n - head) / PER;
+    const size_t body_end = head + nvec * PER;
+    const uint4* __restrict__ vp = reinterpret_cast<const uint4*>(keys + head);
+    const size_t tid = (size_t)blockIdx.x * BLOCK + threadIdx.x, stride = (size_t)gridDim.x * BLOCK;
     unsigned long long c = 0;
-    for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK)
-        c += RK::ordered(keys[i]) < tm ? 1ull : 0ull;
+    if (tid < head) c += RK::ordered(keys[tid]) < tm ? 1ull : 0ull;
+    for (size_t i = tid; i < nvec; i += 4 * stride) {
+        uint4 q[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (i + u * stride < nvec) q[u] = vp[i + u * stride];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (i + u * stride >= nvec) continue;
+            union { uint4 v; KB k[PER]; } w;
+            w.v = q[u];
+#pragma unroll
+            for (int e = 0; e < PER; e++) c += RK::ordered(w.k[e]) < tm ? 1ull : 0ull;
+        }
+    }
+    if (body_end + tid < n) c += RK::ordered(keys[body_end + tid]) < tm ? 1ull : 0ull;  // tail < PER elements
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(0xffffffffu, c, d);
     if ((threadIdx.x & 31u) == 0 && c) atomicAdd(&ctrl->rot_count, c);

@@ -106,7 +106,7 @@ static bool radix_sort_run(K* keys, V* vals0, size_t n, cudaStream_t s, int vals
                 cur ^= 1;
                 m = nb;
             }
-            radix_count_below_kernel<K, 256><<<(unsigned)(sms * 4), 256, 0, s>>>((const KB*)keys, n, ti[cur], ctrl);
+            radix_count_below_kernel<K, 256><<<(unsigned)(sms * 8), 256, 0, s>>>((const KB*)keys, n, ti[cur], ctrl);
             count_launch();
             ktimer_mark("radix_nan_rotation", s);
         }
