@@ -245,6 +245,36 @@ def test_scan_by_key(N, kname, vname):
                 assert got.tobytes() == exp.tobytes(), (kname, vname, n, excl)
 
 
+@pytest.mark.parametrize("kname,vname", [("int32_t", "int32_t"), ("int64_t", "int64_t")])
+def test_scan_by_key_long_runs_inplace_unaligned(N, kname, vname):
+    # segments spanning many tiles (the segmented look-back walks over head-free tiles),
+    # a single segment, all heads, in-place output, and arrays shifted off 16-byte alignment
+    rng = np.random.default_rng(31)
+    n = (1 << 21) + 37
+    cases = {
+        "long runs": np.repeat(np.arange(40), rng.multinomial(n, [1 / 40] * 40)),
+        "one segment": np.zeros(n, np.int64),
+        "all heads": np.arange(n),
+    }
+    for label, kk in cases.items():
+        keys = kk[:n].astype(NP_OF[kname])
+        vals = rng.integers(-1000, 1000, n).astype(NP_OF[vname])
+        for excl in (False, True):
+            ini = np.array([7], NP_OF[vname])
+            exp = O.scan_by_key(keys, vals, "Plus", excl, 7 if excl else None)
+            for shift in (0, 1):
+                dk = dev(np.concatenate([np.zeros(shift, keys.dtype), keys]))
+                dv = dev(np.concatenate([np.zeros(shift, vals.dtype), vals]))
+                esz = keys.dtype.itemsize
+                kp = ctypes.c_void_p(dk.data_ptr() + shift * esz)
+                vp = ctypes.c_void_p(dv.data_ptr() + shift * esz)
+                rc = N.lib.trtc_raw_scan_by_key(N.TYPE_CODES[kname], N.TYPE_CODES[vname], int(excl), kp, vp, vp, n,
+                                                ini.ctypes.data_as(ctypes.c_void_p), None)
+                assert rc == 0, N.last_error()
+                got = host(dv, NP_OF[vname])[shift:]
+                assert got.tobytes() == exp.tobytes(), (label, excl, shift)
+
+
 @pytest.mark.parametrize("name", ["int32_t", "float", "uint8_t", "int64_t"])
 def test_remove_unique(N, name):
     rng = np.random.default_rng(29)

@@ -861,6 +861,260 @@ __global__ void __launch_bounds__(BLOCK) scan_by_key_kernel(KV keys, InV vals, O
     }
 }
 
+// ---------------------------------------------------------------- two-phase segmented scan
+// scan_by_key for contiguous keys and values of one element size (4 or 8 bytes) under the
+// built-in EqualTo / Plus, in the persistent software-pipelined form of scan2_kernel:
+// phase 1 reads a tile (16-byte loads of keys and values) and publishes its segmented
+// aggregate -- the sum after its last segment head, with a head flag -- phase 2 looks back
+// (segmented: the walk stops at the first tile holding a head), re-reads the tile (normally
+// from L2) and writes it.  No tile data is held in registers across a wait.  Elements past
+// n (last tile) or every element of unaligned arrays take scalar loads; elements past n
+// count as heads of value T() and are not stored, so they never reach a valid output.
+#ifndef TRTC_SBK2_MINB
+#define TRTC_SBK2_MINB 5  // resident CTAs per SM the kernel is compiled for (B200 sweep: 1 -> 1.36 ms, 5 -> 0.99 ms at 2^28)
+#endif
+template <class K, class T, int MODE, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __restrict__ keys, const T* vals, T* out,
+                                                                     size_t n, size_t tiles, T init, LookbackState st) {
+    static_assert(sizeof(K) == sizeof(T) && (sizeof(T) == 4 || sizeof(T) == 8), "keys and values of one width");
+    constexpr int VEC = VecWidth<T>::V;
+    static_assert(ITEMS % VEC == 0, "whole 16-byte vectors per lane");
+    constexpr int ROWS = ITEMS / VEC;
+    constexpr int WARPS = BLOCK / 32;
+    constexpr int WSEG = 32 * ITEMS;
+    constexpr int TILE = BLOCK * ITEMS;
+    typedef union { uint4 q; T t[VEC]; } VecT;
+    typedef union { uint4 q; K k[VEC]; } VecK;
+    __shared__ unsigned long long s_ticket;
+    __shared__ T s_wtot[2][WARPS];
+    __shared__ int s_whd[2][WARPS];
+    __shared__ T s_woff[2][WARPS];
+    __shared__ int s_woh[2][WARPS], s_wohd[2][WARPS];
+    __shared__ T s_agg[2];
+    __shared__ int s_agg_hd[2];
+    __shared__ T s_pre;
+    __shared__ int s_pre_h;
+    Plus op;
+    EqualTo eq;
+
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const bool aligned = ((((size_t)keys) | ((size_t)vals) | ((size_t)out)) & 15) == 0;
+
+    auto claim = [&]() -> size_t {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned long long t = atomicAdd(st.tile_ctr, 1ull);
+            if (t == (unsigned long long)tiles + gridDim.x - 1) atomicExch(st.tile_ctr, 0ull);
+            s_ticket = t;
+        }
+        __syncthreads();
+        return (size_t)s_ticket;
+    };
+    // fast rows are loaded up front (all 16-byte loads of the warp segment in flight at once)
+    auto preload = [&](size_t wstart, bool phase2, VecK (&kq)[ROWS], VecT (&vq)[ROWS]) {
+#pragma unroll
+        for (int r = 0; r < ROWS; r++) {
+            const size_t i0 = wstart + (size_t)r * 32 * VEC + (size_t)lane * VEC;
+            kq[r].q = reinterpret_cast<const uint4*>(keys + i0)[0];
+            vq[r].q = phase2 ? __ldcs(reinterpret_cast<const uint4*>(vals + i0)) : reinterpret_cast<const uint4*>(vals + i0)[0];
+        }
+    };
+    // one row of the warp's segment: lane l holds elements wstart + r*32*VEC + l*VEC + e;
+    // hd[e]: element e starts a segment; prevk_row: key before the row's first element
+    auto load_row = [&](size_t wstart, int r, bool fast, K prevk_row, const VecK& kq, const VecT& vq, K (&k)[VEC],
+                        T (&x)[VEC], bool (&hd)[VEC]) {
+        const size_t i0 = wstart + (size_t)r * 32 * VEC + (size_t)lane * VEC;
+        if (fast) {
+#pragma unroll
+            for (int e = 0; e < VEC; e++) { k[e] = kq.k[e]; x[e] = vq.t[e]; }
+        } else {
+#pragma unroll
+            for (int e = 0; e < VEC; e++) {
+                const bool ok = i0 + e < n;
+                k[e] = ok ? keys[i0 + e] : K();
+                x[e] = ok ? vals[i0 + e] : T();
+            }
+        }
+        K pk = shfl_up_any(k[VEC - 1], 1);
+        if (lane == 0) pk = prevk_row;
+#pragma unroll
+        for (int e = 0; e < VEC; e++) {
+            const size_t gi = i0 + e;
+            const K before = e == 0 ? pk : k[e - 1];
+            hd[e] = gi == 0 || gi >= n || !(bool)eq(before, k[e]);
+        }
+    };
+    auto first_key = [&](size_t wstart) -> K { return wstart > 0 && wstart - 1 < n ? keys[wstart - 1] : K(); };
+
+    // ---- phase 1: segmented warp aggregates (ordered), tile aggregate, publication
+    auto phase1 = [&](size_t tile, int b) {
+        const size_t wstart = tile * (size_t)TILE + (size_t)warp * WSEG;
+        const bool fast = aligned && wstart + WSEG <= n;
+        K prevk = first_key(wstart);
+        T wt = T();
+        bool wt_h = false, wt_hd = false;
+        VecK kq[ROWS];
+        VecT vq[ROWS];
+        if (fast) preload(wstart, false, kq, vq);
+#pragma unroll
+        for (int r = 0; r < ROWS; r++) {
+            K k[VEC];
+            T x[VEC];
+            bool hd[VEC];
+            load_row(wstart, r, fast, prevk, kq[r], vq[r], k, x, hd);
+            prevk = shfl_any(k[VEC - 1], 31);
+            // lane fold (value after the lane's last head)
+            T a = x[0];
+            bool ahd = hd[0];
+#pragma unroll
+            for (int e = 1; e < VEC; e++) {
+                if (hd[e]) { a = x[e]; ahd = true; }
+                else a = (T)op(a, x[e]);
+            }
+            // ordered tree: lane l combines l (older) and l + d (newer)
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const T o = shfl_down_any(a, d);
+                const int ohd = __shfl_down_sync(0xffffffffu, (int)ahd, d);
+                if ((lane & (2 * d - 1)) == 0 && lane + d < 32) {
+                    a = ohd ? o : (T)op(a, o);
+                    ahd = ahd || ohd;
+                }
+            }
+            a = shfl_any(a, 0);
+            ahd = __shfl_sync(0xffffffffu, (int)ahd, 0) != 0;
+            if (!wt_h || ahd) wt = a;
+            else wt = (T)op(wt, a);
+            wt_h = true;
+            wt_hd = wt_hd || ahd;
+        }
+        if (lane == 0) { s_wtot[b][warp] = wt; s_whd[b][warp] = wt_hd ? 1 : 0; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            T agg = T();
+            bool agg_h = false, agg_hd = false;
+            for (int w = 0; w < WARPS; w++) {
+                s_woff[b][w] = agg;
+                s_woh[b][w] = agg_h ? 1 : 0;
+                s_wohd[b][w] = agg_hd ? 1 : 0;
+                const bool whd = s_whd[b][w] != 0;
+                agg = (!agg_h || whd) ? s_wtot[b][w] : (T)op(agg, s_wtot[b][w]);
+                agg_h = true;
+                agg_hd = agg_hd || whd;
+            }
+            s_agg[b] = agg;
+            s_agg_hd[b] = agg_hd ? 1 : 0;
+            publish<T>(st, tile, agg, tile == 0, agg_hd);
+        }
+    };
+
+    size_t cur = claim();
+    if (cur >= tiles) return;
+    int buf = 0;
+    phase1(cur, 0);
+    while (true) {
+        const size_t nxt = claim();
+        if (nxt < tiles) phase1(nxt, buf ^ 1);
+        // segmented look-back of the current tile (warp 0): the running segment value entering it
+        if (warp == 0) {
+            T tp = T();
+            bool tp_h = false;
+            if (cur > 0) {
+                bool tp_hd = false;
+                const Opt<T> p = lookback_prefix<T, Plus, true>(st, cur, op, tp_hd);
+                tp = p.v;
+                tp_h = p.h;
+                T incl = tp;
+                if (s_agg_hd[buf] || !tp_h) incl = s_agg[buf];
+                else incl = (T)op(tp, s_agg[buf]);
+                if (lane == 0) publish<T>(st, cur, incl, true, tp_hd || s_agg_hd[buf] != 0);
+            }
+            if (lane == 0) { s_pre = tp; s_pre_h = tp_h ? 1 : 0; }
+        }
+        __syncthreads();
+        // re-read and write the current tile
+        {
+            const size_t wstart = cur * (size_t)TILE + (size_t)warp * WSEG;
+            const bool fast = aligned && wstart + WSEG <= n;
+            // carry into the warp = tile prefix, then the tile's earlier warps (segmented)
+            T carry = s_pre;
+            bool carry_h = s_pre_h != 0;
+            if (s_woh[buf][warp]) {
+                if (s_wohd[buf][warp] || !carry_h) carry = s_woff[buf][warp];
+                else carry = (T)op(carry, s_woff[buf][warp]);
+                carry_h = true;
+            }
+            K prevk = first_key(wstart);
+            VecK kq[ROWS];
+            VecT vq[ROWS];
+            if (fast) preload(wstart, true, kq, vq);
+#pragma unroll
+            for (int r = 0; r < ROWS; r++) {
+                K k[VEC];
+                T x[VEC];
+                bool hd[VEC];
+                load_row(wstart, r, fast, prevk, kq[r], vq[r], k, x, hd);
+                prevk = shfl_any(k[VEC - 1], 31);
+                T a = x[0];
+                bool ahd = hd[0];
+#pragma unroll
+                for (int e = 1; e < VEC; e++) {
+                    if (hd[e]) { a = x[e]; ahd = true; }
+                    else a = (T)op(a, x[e]);
+                }
+                // inclusive segmented scan over the lanes
+                T inc = a;
+                bool ihd = ahd;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const T y = shfl_up_any(inc, d);
+                    const int yhd = __shfl_up_sync(0xffffffffu, (int)ihd, d);
+                    if (lane >= (uint32_t)d) {
+                        if (!ihd) inc = (T)op(y, inc);
+                        ihd = ihd || yhd;
+                    }
+                }
+                const T ex = shfl_up_any(inc, 1);
+                const bool exhd = __shfl_up_sync(0xffffffffu, (int)ihd, 1) != 0;
+                const T row_tot = shfl_any(inc, 31);
+                const bool row_hd = __shfl_sync(0xffffffffu, (int)ihd, 31) != 0;
+                // running value entering this lane's first element
+                T run = carry;
+                bool run_h = carry_h;
+                if (lane > 0) {
+                    run = (exhd || !run_h) ? ex : (T)op(run, ex);
+                    run_h = true;
+                }
+                T y[VEC];
+#pragma unroll
+                for (int e = 0; e < VEC; e++) {
+                    const T c = hd[e] ? x[e] : (run_h ? (T)op(run, x[e]) : x[e]);
+                    if (MODE == 0) y[e] = c;
+                    else y[e] = hd[e] ? init : (T)op(init, run);
+                    run = c;
+                    run_h = true;
+                }
+                const size_t i0 = wstart + (size_t)r * 32 * VEC + (size_t)lane * VEC;
+                if (fast) {
+                    VecT o;
+#pragma unroll
+                    for (int e = 0; e < VEC; e++) o.t[e] = y[e];
+                    __stcs(reinterpret_cast<uint4*>(out + i0), o.q);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < VEC; e++)
+                        if (i0 + e < n) out[i0 + e] = y[e];
+                }
+                carry = (row_hd || !carry_h) ? row_tot : (T)op(carry, row_tot);
+                carry_h = true;
+            }
+        }
+        if (nxt >= tiles) break;
+        cur = nxt;
+        buf ^= 1;
+    }
+}
+
 // ---------------------------------------------------------------- commutative reduce
 // Built-in commutative operators over contiguous input: 16-byte loads, VEC independent
 // per-thread accumulators (shorter FP accumulation chains), warp/block trees, one partial

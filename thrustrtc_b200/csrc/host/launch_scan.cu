@@ -161,8 +161,38 @@ bool reduce_raw(int tc, int op, const void* in, size_t n, const void* init, void
 }
 
 // ---------------------------------------------------------------- scan_by_key
+#ifndef TRTC_SBK2
+#define TRTC_SBK2 1  // two-phase segmented scan for keys and values of one width
+#endif
+#ifndef TRTC_SBK2_ITEMS
+#define TRTC_SBK2_ITEMS 8  // elements per thread of a two-phase segmented-scan tile (4-byte types)
+#endif
+
 template <class K, class T, int MODE>
 static bool sbk_t(const K* keys, const T* vals, T* out, size_t n, const T* init, cudaStream_t s) {
+    const bool out_over_keys = (const void*)out < (const void*)(keys + n) && (const void*)keys < (const void*)(out + n);
+    if constexpr (TRTC_SBK2 && sizeof(K) == sizeof(T) && (sizeof(T) == 4 || sizeof(T) == 8)) {
+        if (!out_over_keys) {
+            constexpr int ITEMS = TRTC_SBK2_ITEMS * 4 / (int)sizeof(T) < VecWidth<T>::V
+                                      ? VecWidth<T>::V : TRTC_SBK2_ITEMS * 4 / (int)sizeof(T);
+            constexpr int TILE = SCAN_BLOCK * ITEMS;
+            const size_t tiles = (n + TILE - 1) / TILE;
+            LookbackState st;
+            if (!fill_lookback(st, s, tiles, sizeof(T), true)) return false;
+            // persistent CTAs: as many as fit on the device at once
+            auto kernel = sbk2_kernel<K, T, MODE, SCAN_BLOCK, ITEMS>;
+            static int per_sm = 0;
+            if (per_sm == 0 && !TRTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, SCAN_BLOCK, 0)))
+                return false;
+            size_t grid = (size_t)(per_sm > 0 ? per_sm : 1) * sm_count();
+            if (grid > tiles) grid = tiles;
+            ktimer_mark("", s);
+            kernel<<<(unsigned)grid, SCAN_BLOCK, 0, s>>>(keys, vals, out, n, tiles, init ? *init : T(), st);
+            count_launch();
+            ktimer_mark("scan_by_key_kernel", s);
+            return TRTC_CUDA(cudaGetLastError());
+        }
+    }
     constexpr int VK = VecWidth<K>::V, VT = VecWidth<T>::V;
     constexpr int VEC = VK > VT ? VK : VT;
     constexpr int NV = VEC >= 8 ? 2 : 4;
