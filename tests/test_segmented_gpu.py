@@ -87,6 +87,7 @@ def test_segmented_matches_per_segment_sort_and_scan(N, name, desc):
     lens = make_lengths(rng, 400, 64, 1.5, 20000)
     lens[:5] = [0, 1, 2, 2048, 4097]     # empty, single, tile edges of both configurations
     lens[5:8] = [4096, 4095, 12000]       # on-chip limit and a chunked segment
+    lens[8:20] = [31, 32, 33, 255, 256, 257, 511, 512, 513, 300, 700, 3]  # one-warp limits (256 / 512 keys)
     off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
     n = int(off[-1])
     keys = keys_for(rng, name, n)

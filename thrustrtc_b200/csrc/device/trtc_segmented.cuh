@@ -141,6 +141,107 @@ __device__ inline V seg_block_excl_scan(const V* s_v, V* s_o, uint32_t len, V ca
     return total;
 }
 
+// One warp sorts (stable LSD, 8-bit digits) and scans a segment of len <= 32 * ITEMS keys on
+// its own: no block barrier, so the CTA's eight warps work on eight small segments at once.
+// Element e = i*32 + lane sits in item i of the lane; sk / sv are this warp's staging slices
+// (32 * ITEMS elements), wh its 256 digit counters.
+template <class K, class V, bool DESC, int ITEMS>
+__device__ inline void seg_warp_sort_scan(typename RadixKey<K>::B* gk, V* gv, V* gs, uint32_t len,
+                                          typename RadixKey<K>::B* sk, V* sv, uint32_t* wh) {
+    typedef typename RadixKey<K>::B KB;
+    constexpr int D = RadixKey<K>::DIGITS;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int IT = (int)((len + 31u) / 32u);  // items in use (warp-uniform)
+    const uint32_t ltm = lanemask_lt();
+    KB k[ITEMS];
+    V v[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const uint32_t e = (uint32_t)i * 32u + lane;
+        if (i < IT && e < len) { k[i] = gk[e]; v[i] = gv[e]; }
+        else { k[i] = KB(0); v[i] = V(); }
+    }
+    for (int p = 0; p < D; p++) {
+        const uint32_t sel = 0x4440u | (uint32_t)(p & 3);
+        const bool hi = p >= 4;
+#pragma unroll
+        for (int j = 0; j < 8; j++) wh[j * 32 + lane] = 0;
+        __syncwarp();
+        uint32_t pos[ITEMS], info[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            pos[i] = 0;
+            info[i] = 0;
+            if (i >= IT) continue;
+            const bool valid = (uint32_t)i * 32u + lane < len;
+            const uint32_t d = radix_digit_sel<K, DESC>(k[i], sel, hi);
+            uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                const bool set = (d >> b) & 1u;
+                const uint32_t bb = __ballot_sync(0xffffffffu, set);
+                peers &= set ? bb : ~bb;
+            }
+            const uint32_t leader = 31u - __clz(peers | 1u);
+            info[i] = (uint32_t)__popc(peers & ltm) | (leader << 8);
+            if (valid && lane == leader) pos[i] = atomicAdd(&wh[d], (uint32_t)__popc(peers));
+        }
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++)
+            if (i < IT) pos[i] = __shfl_sync(0xffffffffu, pos[i], (int)(info[i] >> 8)) + (info[i] & 0xFFu);
+        __syncwarp();
+        // exclusive scan of the 256 counters: lane owns digits 8*lane .. 8*lane+7
+        uint32_t c[8], sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) { c[j] = wh[lane * 8 + j]; sum += c[j]; }
+        uint32_t inc = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= (uint32_t)d) inc += y;
+        }
+        uint32_t run = inc - sum;
+#pragma unroll
+        for (int j = 0; j < 8; j++) { wh[lane * 8 + j] = run; run += c[j]; }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            if (i >= IT || (uint32_t)i * 32u + lane >= len) continue;
+            const uint32_t q = pos[i] + wh[radix_digit_sel<K, DESC>(k[i], sel, hi)];
+            sk[q] = k[i];
+            sv[q] = v[i];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t e = (uint32_t)i * 32u + lane;
+            if (i < IT && e < len) { k[i] = sk[e]; v[i] = sv[e]; }
+        }
+        __syncwarp();
+    }
+    // exclusive scan of the sorted values, written with the sorted keys and values
+    V carry = V();
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        if (i >= IT) continue;
+        const uint32_t e = (uint32_t)i * 32u + lane;
+        const bool valid = e < len;
+        const V x = valid ? v[i] : V();
+        V incl = x;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const V y = shfl_up_any(incl, d);
+            if (lane >= (uint32_t)d) incl += y;
+        }
+        if (valid) {
+            gk[e] = k[i];
+            gv[e] = v[i];
+            if (gs) gs[e] = carry + incl - x;
+        }
+        carry += shfl_any(incl, 31);
+    }
+}
+
 template <class K, class V, int ITEMS>
 constexpr size_t seg_sort_scan_smem() {
     return (size_t)256 * ITEMS * (2 * sizeof(V) + sizeof(typename RadixKey<K>::B)) + 8 * 256 * 4;
@@ -170,19 +271,12 @@ __global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey
     __shared__ uint32_t s_wsum[8];
     __shared__ V s_part[8];
     __shared__ unsigned long long s_item;
+    __shared__ unsigned long long s_batch, s_defer[8];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    constexpr uint32_t WSEG = 32u * ITEMS;  // segments up to this length are sorted by one warp
 
-    while (true) {
-        __syncthreads();
-        if (threadIdx.x == 0) s_item = atomicAdd(&ctrl->next, 1ull);
-        __syncthreads();
-        const unsigned long long item = s_item;
-        if (item >= nseg) return;
-        KB* gk;
-        V* gv;
-        V* gs;
-        uint32_t len;
-        unsigned long long base;
+    // the arrays and length of queue entry `item`
+    auto fetch = [&](unsigned long long item, KB*& gk, V*& gv, V*& gs, uint32_t& len, unsigned long long& base) {
         if (items) {  // list mode: segments in queue order, each with its own arrays
             const SegItem it = items[item];
             gk = reinterpret_cast<KB*>(it.k);
@@ -198,8 +292,10 @@ __global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey
             gv = vals + base;
             gs = scan + base;
         }
-        if (len == 0) continue;
+    };
 
+    // whole-CTA sort + scan of one segment (on chip up to TILE keys, else through global memory)
+    auto block_segment = [&](KB* gk, V* gv, V* gs, uint32_t len, unsigned long long base) {
         if (len <= (uint32_t)TILE) {
             // ---------------- on-chip sort of a small segment
             const int IT = (int)((len + 255u) / 256u);
@@ -238,7 +334,7 @@ __global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey
                 gv[e] = s_v[e];
                 if (gs) gs[e] = s_o[e];
             }
-            continue;
+            return;
         }
 
         // ---------------- large segment: CTA-level LSD passes through global memory
@@ -313,6 +409,53 @@ __global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey
                 carry = seg_block_excl_scan<V, ITEMS>(s_v, s_o, cn, carry, s_part);
                 for (uint32_t e = threadIdx.x; e < cn; e += 256) gs[cb + e] = s_o[e];
             }
+            __syncthreads();
+        }
+    };
+
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctrl->next, 1ull);
+        __syncthreads();
+        const unsigned long long item = s_item;
+        if (item >= nseg) return;
+        KB* gk;
+        V* gv;
+        V* gs;
+        uint32_t len;
+        unsigned long long base;
+        fetch(item, gk, gv, gs, len, base);
+        if (len == 0) continue;
+        if (len > WSEG) {
+            block_segment(gk, gv, gs, len, base);
+            continue;
+        }
+        // a small segment: the queue has handed out every large one already, so take seven
+        // more entries and let each warp sort one; entries longer than a warp's share are
+        // deferred to the whole CTA afterwards
+        if (threadIdx.x == 0) s_batch = atomicAdd(&ctrl->next, 7ull);
+        __syncthreads();
+        const unsigned long long mine = warp == 0 ? item : s_batch + warp - 1;
+        unsigned long long defer = ~0ull;
+        if (mine < nseg) {
+            KB* wk;
+            V* wv;
+            V* ws;
+            uint32_t wl;
+            unsigned long long wb;
+            fetch(mine, wk, wv, ws, wl, wb);
+            if (wl > WSEG) defer = mine;
+            else if (wl > 0)
+                seg_warp_sort_scan<K, V, DESC, ITEMS>(wk, wv, ws, wl, s_k + warp * WSEG, s_v + warp * WSEG,
+                                                      s_whist + warp * 256);
+        }
+        if (lane == 0) s_defer[warp] = defer;
+        __syncthreads();
+        for (int w = 0; w < 8; w++) {
+            const unsigned long long d = s_defer[w];
+            if (d == ~0ull) continue;
+            fetch(d, gk, gv, gs, len, base);
+            block_segment(gk, gv, gs, len, base);
             __syncthreads();
         }
     }
