@@ -870,8 +870,11 @@ __global__ void __launch_bounds__(BLOCK) scan_by_key_kernel(KV keys, InV vals, O
 // from L2) and writes it.  No tile data is held in registers across a wait.  Elements past
 // n (last tile) or every element of unaligned arrays take scalar loads; elements past n
 // count as heads of value T() and are not stored, so they never reach a valid output.
+#ifndef TRTC_SBK2_AHEAD
+#define TRTC_SBK2_AHEAD 0  // draw the next tile's ticket during the look-back instead of after
+#endif
 #ifndef TRTC_SBK2_MINB
-#define TRTC_SBK2_MINB 5  // resident CTAs per SM the kernel is compiled for (B200 sweep: 1 -> 1.36 ms, 5 -> 0.99 ms at 2^28)
+#define TRTC_SBK2_MINB 4  // resident CTAs per SM the kernel is compiled for
 #endif
 template <class K, class T, int MODE, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __restrict__ keys, const T* vals, T* out,
@@ -939,10 +942,11 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
         if (lane == 0) pk = prevk_row;
 #pragma unroll
         for (int e = 0; e < VEC; e++) {
-            const size_t gi = i0 + e;
             const K before = e == 0 ? pk : k[e - 1];
-            hd[e] = gi == 0 || gi >= n || !(bool)eq(before, k[e]);
+            hd[e] = !(bool)eq(before, k[e]);
+            if (!fast) hd[e] = hd[e] || i0 + e >= n;
         }
+        if (i0 == 0) hd[0] = true;
     };
     auto first_key = [&](size_t wstart) -> K { return wstart > 0 && wstart - 1 < n ? keys[wstart - 1] : K(); };
 
@@ -971,18 +975,14 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
                 if (hd[e]) { a = x[e]; ahd = true; }
                 else a = (T)op(a, x[e]);
             }
-            // ordered tree: lane l combines l (older) and l + d (newer)
+            // the row's value after its last head: the lanes from the last lane holding a
+            // head (lane 0 when none) summed by a butterfly (Plus, T() its identity)
+            const uint32_t hm = __ballot_sync(0xffffffffu, ahd);
+            const uint32_t last = hm ? 31u - __clz(hm) : 0u;
+            a = lane >= last ? a : T();
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const T o = shfl_down_any(a, d);
-                const int ohd = __shfl_down_sync(0xffffffffu, (int)ahd, d);
-                if ((lane & (2 * d - 1)) == 0 && lane + d < 32) {
-                    a = ohd ? o : (T)op(a, o);
-                    ahd = ahd || ohd;
-                }
-            }
-            a = shfl_any(a, 0);
-            ahd = __shfl_sync(0xffffffffu, (int)ahd, 0) != 0;
+            for (int d = 16; d > 0; d >>= 1) a = (T)op(a, shfl_xor_any(a, d));
+            ahd = hm != 0;
             if (!wt_h || ahd) wt = a;
             else wt = (T)op(wt, a);
             wt_h = true;
@@ -1012,8 +1012,16 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
     if (cur >= tiles) return;
     int buf = 0;
     phase1(cur, 0);
+#if TRTC_SBK2_AHEAD
+    // the ticket after next is drawn by thread 0 during the look-back (its latency then hides
+    // behind the look-back's) and read after the barrier that follows it; a CTA stops drawing
+    // once it holds a ticket >= tiles, so each CTA still takes exactly one such ticket
+    size_t nxt = claim();
+#endif
     while (true) {
+#if !TRTC_SBK2_AHEAD
         const size_t nxt = claim();
+#endif
         if (nxt < tiles) phase1(nxt, buf ^ 1);
         // segmented look-back of the current tile (warp 0): the running segment value entering it
         if (warp == 0) {
@@ -1030,8 +1038,21 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
                 if (lane == 0) publish<T>(st, cur, incl, true, tp_hd || s_agg_hd[buf] != 0);
             }
             if (lane == 0) { s_pre = tp; s_pre_h = tp_h ? 1 : 0; }
+#if TRTC_SBK2_AHEAD
+            if (lane == 0) {
+                unsigned long long t = ~0ull;
+                if (nxt < tiles) {
+                    t = atomicAdd(st.tile_ctr, 1ull);
+                    if (t == (unsigned long long)tiles + gridDim.x - 1) atomicExch(st.tile_ctr, 0ull);
+                }
+                s_ticket = t;
+            }
+#endif
         }
         __syncthreads();
+#if TRTC_SBK2_AHEAD
+        const size_t nxt2 = (size_t)s_ticket;
+#endif
         // re-read and write the current tile
         {
             const size_t wstart = cur * (size_t)TILE + (size_t)warp * WSEG;
@@ -1062,22 +1083,23 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
                     if (hd[e]) { a = x[e]; ahd = true; }
                     else a = (T)op(a, x[e]);
                 }
-                // inclusive segmented scan over the lanes
+                // inclusive segmented scan over the lanes: at distance d, lane l holds lanes
+                // (l-d, l] and takes in (l-2d, l-d] only if no lane of its window holds a head
+                const uint32_t hm = __ballot_sync(0xffffffffu, ahd);
+                const uint32_t le = lane == 31u ? 0xffffffffu : ((2u << lane) - 1u);  // lanes <= l
                 T inc = a;
-                bool ihd = ahd;
 #pragma unroll
                 for (int d = 1; d < 32; d <<= 1) {
                     const T y = shfl_up_any(inc, d);
-                    const int yhd = __shfl_up_sync(0xffffffffu, (int)ihd, d);
                     if (lane >= (uint32_t)d) {
-                        if (!ihd) inc = (T)op(y, inc);
-                        ihd = ihd || yhd;
+                        const uint32_t win = le & ~((1u << (lane - (uint32_t)d + 1u)) - 1u);
+                        if ((hm & win) == 0u) inc = (T)op(y, inc);
                     }
                 }
                 const T ex = shfl_up_any(inc, 1);
-                const bool exhd = __shfl_up_sync(0xffffffffu, (int)ihd, 1) != 0;
+                const bool exhd = (hm & (le >> 1)) != 0u;  // a head in lanes < l
                 const T row_tot = shfl_any(inc, 31);
-                const bool row_hd = __shfl_sync(0xffffffffu, (int)ihd, 31) != 0;
+                const bool row_hd = hm != 0u;
                 // running value entering this lane's first element
                 T run = carry;
                 bool run_h = carry_h;
@@ -1111,6 +1133,9 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
         }
         if (nxt >= tiles) break;
         cur = nxt;
+#if TRTC_SBK2_AHEAD
+        nxt = nxt2;
+#endif
         buf ^= 1;
     }
 }
