@@ -252,6 +252,22 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
     const char* ib = (const char*)in;
     const char* ob = (const char*)out;
     const bool disjoint = ob + n * sizeof(T) <= ib || ib + n * sizeof(T) <= ob;
+    if (!disjoint) {
+        // in place: the two-phase kernel into a pool temporary, then the kept elements copied
+        // back (2^28 i32, half kept: 0.42 + 0.17 ms against 1.06 ms for the one-pass kernel);
+        // the one-pass kernel remains for when no temporary can be had
+        T* tmp = (T*)tmp_alloc(n * sizeof(T), s);
+        if (tmp) {
+            unsigned long long c = 0;
+            bool ok = compact_t<T, MODE, CT>(in, tmp, n, value, s, &c);
+            if (ok && c > 0)
+                ok = TRTC_CUDA(cudaMemcpyAsync(out, tmp, (size_t)c * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            tmp_free(tmp, s);
+            *count = c;
+            return ok;
+        }
+        (void)cudaGetLastError();  // the failed allocation must not fail the launch check below
+    }
     constexpr int ITEMS1 = 16, ITEMS2 = TRTC_COMPACT2_ITEMS;
     const int ITEMS = disjoint ? ITEMS2 : ITEMS1;
     const size_t TILE = (size_t)SCAN_BLOCK * ITEMS;

@@ -518,6 +518,28 @@ unsigned long long run_compact(CompactSpec& c) {
     const std::string ptype = c.pred ? c.pred->name_view_cls() : "EqualTo";
     const ViewBuf pbytes = c.pred ? c.pred->view() : nothing_bytes();
     const bool two_phase = c.disjoint();
+    if (!two_phase && !c.partition && !c.two && c.written.size() == 1 && c.written[0]->contiguous_data() &&
+        c.in->contiguous_data() && (!c.stencil || c.stencil->contiguous_data())) {
+        // in place (one contiguous output overlapping the input): the two-phase kernel into a
+        // pool temporary, then the kept elements copied back; the one-pass kernel remains for
+        // views and multi-output forms, or when no temporary can be had
+        const DVVectorLike* o = c.written[0];
+        void* tmp = tmp_alloc(n * o->elem_size(), S());
+        if (tmp) {
+            CompactSpec t = c;
+            t.out = raw_view(tmp, n, o->name_elem_cls());
+            t.written.clear();
+            const unsigned long long cnt = run_compact(t);
+            bool ok = cnt != kFail;
+            const size_t keep = cnt == kFail ? 0 : (size_t)std::min<unsigned long long>(cnt, o->size());
+            if (ok && keep > 0)
+                ok = TRTC_CUDA(cudaMemcpyAsync(o->contiguous_data(), tmp, keep * o->elem_size(), cudaMemcpyDeviceToDevice,
+                                               S()));
+            tmp_free(tmp, S());
+            return ok ? cnt : kFail;
+        }
+        (void)cudaGetLastError();  // the failed allocation must not fail a later launch check
+    }
     const size_t tile = 256 * (two_phase ? 32 : 16);
     const size_t tiles = (n + tile - 1) / tile;
     ViewBuf st;
