@@ -49,3 +49,27 @@ def test_no_exit_calls_in_library():
     except (OSError, subprocess.CalledProcessError):
         pytest.skip("objdump not available")
     assert "<exit@plt>" not in "\n".join(l for l in dis.splitlines() if "call" in l)
+
+
+def test_python_names_of_the_reference_package():
+    # every public name of python/ThrustRTC/*.py is importable from the package
+    import thrustrtc_b200 as t
+    names = ["DVCupyVector", "DVNumbaVector", "Dim3", "ObjArray", "StrArray", "ValueFromDVPtr", "DVTorchVector",
+             "Sort_By_Key", "Merge_By_Key", "Inner_Product", "Partition_Point", "Is_Sorted_Until", "DVZipped",
+             "DVCustomVector", "DVTuple", "Tabulate", "Adjacent_Difference"]
+    assert [n for n in names if not hasattr(t, n)] == []
+
+
+def test_cuda_array_interface_adaptor_checks_dtype_and_contiguity():
+    import pytest
+    import thrustrtc_b200 as t
+
+    class Fake:
+        def __init__(self, typestr, shape, strides=None):
+            self.__cuda_array_interface__ = {"data": (0, False), "typestr": typestr, "shape": shape,
+                                             "strides": strides, "version": 3}
+
+    with pytest.raises(ValueError):
+        t.DVCupyVector(Fake("<f2", (4,)))          # float16: no element type of the library
+    with pytest.raises(ValueError):
+        t.DVNumbaVector(Fake("<i4", (4,), (8,)))   # strided

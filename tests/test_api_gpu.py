@@ -395,3 +395,17 @@ def test_sort_by_key_zipped_payload_and_custom_vector(trtc):
     out = trtc.device_vector("int32_t", 1000)
     trtc.Inclusive_Scan(cv, out)
     assert out.to_host().tolist() == np.cumsum(2 * np.arange(1000)).tolist()
+
+
+def test_cuda_array_interface_vectors(trtc):
+    # DVCupyVector / DVNumbaVector adapt any CUDA Array Interface exporter (a torch tensor here)
+    import torch
+    x = torch.tensor([5, 3, 9, 1, 7], dtype=torch.int32, device="cuda")
+    v = trtc.DVCupyVector(x)
+    assert v.name_elem_cls() == "int32_t" and v.size() == 5
+    trtc.Sort(v)
+    torch.cuda.synchronize()
+    assert x.cpu().tolist() == [1, 3, 5, 7, 9]
+    y = torch.tensor([1.5, -2.0, 0.25], dtype=torch.float64, device="cuda")
+    w = trtc.DVNumbaVector(y)
+    assert trtc.Reduce(w) == -0.25

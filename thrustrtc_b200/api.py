@@ -447,6 +447,39 @@ class DVVectorAdaptor(DVVectorLike):
         self.m_cptr = check_cptr(lib.n_dvvectoradaptor_create(elem_cls.encode("utf-8"), size, ptr))
 
 
+class _CudaArrayVector(DVVectorAdaptor):
+    """A non-owning view of any contiguous 1-D device array that exposes the CUDA Array
+    Interface (``__cuda_array_interface__``: CuPy, Numba, PyTorch, ...); keeps a reference."""
+
+    def __init__(self, arr):
+        cai = arr.__cuda_array_interface__
+        dt = np.dtype(cai["typestr"])
+        if dt not in _CLS_OF:
+            raise ValueError("unsupported element type %s" % dt)
+        shape = tuple(cai["shape"])
+        size = int(np.prod(shape)) if shape else 1
+        strides = cai.get("strides")
+        if strides is not None and len(shape) == 1 and strides[0] != dt.itemsize:
+            raise ValueError("the array must be contiguous")
+        DVVectorAdaptor.__init__(self, _CLS_OF[dt], size, ctypes.c_void_p(cai["data"][0]), owner=arr)
+
+
+class DVCupyVector(_CudaArrayVector):
+    """A CuPy device array as a vector (Python DVVector.py:178-212)."""
+
+    def __init__(self, cparr):
+        self.cparr = cparr
+        _CudaArrayVector.__init__(self, cparr)
+
+
+class DVNumbaVector(_CudaArrayVector):
+    """A Numba device array as a vector (Python DVVector.py:141-176)."""
+
+    def __init__(self, nbarr):
+        self.nbarr = nbarr
+        _CudaArrayVector.__init__(self, nbarr)
+
+
 class DVTorchVector(DVVectorAdaptor):
     """Adapts a contiguous 1-D CUDA torch tensor (keeps a reference to it)."""
 
@@ -890,3 +923,11 @@ def Merge(vec1, vec2, vec_out, comp=None):
 def Merge_By_Key(keys1, keys2, value1, value2, keys_out, value_out, comp=None):
     check_i(lib.n_merge_by_key(keys1.m_cptr, keys2.m_cptr, value1.m_cptr, value2.m_cptr, keys_out.m_cptr,
                                value_out.m_cptr, _p(comp)))
+
+
+# ---------------------------------------------------------------- helper names of the reference package
+# (utils.py:3-30, DeviceViewable.py:3-40): argument packers and the value reader
+StrArray = _StrArray
+ObjArray = _ObjArray
+Dim3 = _Dim3
+ValueFromDVPtr = _value_from_dvptr
