@@ -13,9 +13,10 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-# tile edges of the sort (256 x 20 keys for 4-byte keys, 256 x 8 for 8-byte keys) and the scans (4096)
-SIZES = [1, 2, 3, 255, 256, 257, 511, 512, 513, 2047, 2048, 2049, 4095, 4096, 4097, 5119, 5120, 5121, 10241,
-         65537, 1 << 20 | 7]
+# tile edges of the sort (256 x 8 keys for 4-byte keys up to 2^18 keys, 256 x 20 beyond; 256 x 12
+# for 8-byte keys), the switch between the two 4-byte tile sizes, and the scans (4096)
+SIZES = [1, 2, 3, 255, 256, 257, 511, 512, 513, 2047, 2048, 2049, 3071, 3072, 3073, 4095, 4096, 4097, 5119, 5120,
+         5121, 6145, 10241, 65537, 1 << 18, (1 << 18) + 1, 1 << 20 | 7]
 NP_OF = {"int8_t": np.int8, "uint8_t": np.uint8, "int16_t": np.int16, "uint16_t": np.uint16,
          "int32_t": np.int32, "uint32_t": np.uint32, "int64_t": np.int64, "uint64_t": np.uint64,
          "float": np.float32, "double": np.float64}

@@ -13,6 +13,9 @@ namespace trtc_host {
 #ifndef TRTC_RADIX_ITEMS32
 #define TRTC_RADIX_ITEMS32 20
 #endif
+#ifndef TRTC_RADIX_SMALL_N
+#define TRTC_RADIX_SMALL_N (1ull << 18)  // up to this many keys, 4-byte keys use 8-item tiles
+#endif
 #ifndef TRTC_RADIX_ITEMS64
 #define TRTC_RADIX_ITEMS64 12
 #endif
@@ -138,10 +141,16 @@ static bool radix_sort_dispatch(void* keys, void* vals, size_t vsize, size_t n, 
     const bool big = n >= (1ull << 30);
     if (big && sizeof(K) < 4) { set_error("sort: more than 2^30 narrow keys"); return false; }
     K* k = (K*)keys;
+    // small sorts of 4-byte keys take 8-item tiles: a pass over few tiles is bound by one tile's
+    // latency, which shorter ranking loops cut (B200: 2^16 pairs 0.069 -> 0.057 ms, 2^18 0.075 ->
+    // 0.067 ms; from 2^20 up the 20-item tiles are faster)
+    constexpr int SMALL_ITEMS = sizeof(K) == 4 ? 8 : SortTuning<K>::ITEMS;
+    const bool small = n <= TRTC_RADIX_SMALL_N;
 #define TRTC_SORT_RUN(V, HV, vp, fi)                                                                         \
     (big ? radix_sort_run<K, V, HV, DESC, typename trtc::conditional<(sizeof(K) >= 4), unsigned long long, uint32_t>::type>( \
                k, (V*)(vp), n, s, fi)                                                                        \
-         : radix_sort_run<K, V, HV, DESC, uint32_t>(k, (V*)(vp), n, s, fi))
+         : small ? radix_sort_run<K, V, HV, DESC, uint32_t, SMALL_ITEMS>(k, (V*)(vp), n, s, fi)             \
+                 : radix_sort_run<K, V, HV, DESC, uint32_t>(k, (V*)(vp), n, s, fi))
     if (!vals) return TRTC_SORT_RUN(uint32_t, false, nullptr, 0);
     if (vsize == 4) return TRTC_SORT_RUN(uint32_t, true, vals, 0);
     if (vsize == 8) return TRTC_SORT_RUN(unsigned long long, true, vals, 0);
