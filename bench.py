@@ -186,6 +186,25 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def reduce_max(x, world, device):
+    """The maximum of x over all ranks (every rank gets it): the whole job's time is the
+    slowest replica's.  device: where the process group's collectives run (cuda for NCCL,
+    cpu for gloo)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, world, secs_max):
+    """Whole-job throughput of N independent replicas (weak scaling): all ranks' units over
+    the slowest rank's time."""
+    return units_per_rank * world / secs_max
+
+
 def cpu_threads():
     try:
         return max(1, len(os.sched_getaffinity(0)))
@@ -386,11 +405,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, world, dev)
 
     # ---- warm-up
     for _ in range(args.warmup):
@@ -669,12 +684,8 @@ def run_segmented(args):
             ev[i][1].record()
         barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    tot_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = n * world * args.steps / (tot_ms / 1e3) / 1e9
+    tot_ms = reduce_max(sum(step_ms), world, dev)
+    value = replica_rate(n * args.steps, world, tot_ms / 1e3) / 1e9
 
     # correctness of the last replay: per-segment sortedness, stability, scan (size-independent
     # properties over the whole batch, on the device)
