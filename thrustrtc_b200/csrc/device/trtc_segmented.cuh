@@ -250,8 +250,15 @@ constexpr size_t seg_sort_scan_smem() {
 // One persistent launch over the whole batch.  keys/vals: the concatenated segments (sorted
 // in place); scan: receives the exclusive scans; tk/tv: temp arrays of n elements (large
 // segments only).
-template <class K, class V, class OFF, bool DESC, int ITEMS>
-__global__ void __launch_bounds__(256, 2) seg_sort_scan_kernel(typename RadixKey<K>::B* __restrict__ keys,
+// resident CTAs per SM the batched kernel is compiled for (B200, 100k lognormal segments at 8
+// items, u32 keys: 2 CTAs (127 registers) 4.15 ms, 3 CTAs 3.53 ms, 4 CTAs (64 registers) 3.46 ms;
+// 16 items need the shared memory of 3 CTAs; 8-byte keys keep 2 CTAs, which they fill without
+// spilling)
+#ifndef TRTC_SEG_MINB
+#define TRTC_SEG_MINB(items, key_bytes) ((key_bytes) > 4 ? 2 : ((items) <= 8 ? 4 : 3))
+#endif
+template <class K, class V, class OFF, bool DESC, int ITEMS, int MINB = TRTC_SEG_MINB(ITEMS, sizeof(K))>
+__global__ void __launch_bounds__(256, MINB) seg_sort_scan_kernel(typename RadixKey<K>::B* __restrict__ keys,
                                                                 V* __restrict__ vals, V* __restrict__ scan,
                                                                 typename RadixKey<K>::B* __restrict__ tk,
                                                                 V* __restrict__ tv, const OFF* __restrict__ off,
