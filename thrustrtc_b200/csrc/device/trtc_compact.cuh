@@ -136,6 +136,9 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pre
     }
 }
 
+#ifndef TRTC_COMPACT2_MINB
+#define TRTC_COMPACT2_MINB 4  // resident CTAs per SM the two-phase kernel is compiled for
+#endif
 // Two-phase, persistent, software-pipelined form of compact_kernel for outputs that do not
 // overlap the inputs (compiled for 4 resident CTAs per SM, the persistent grid's size): phase 1 reads a tile, evaluates the selection and publishes its count;
 // phase 2 (after the look-back) reads the tile again -- normally from L2 -- and writes it.
@@ -144,7 +147,7 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(InV in, StV stencil, Pre
 // an earlier tile's range before that tile re-reads it.)
 template <int MODE, bool PARTITION, bool TWO, class InV, class StV, class Pred, class ValT, class OutV, class FalseV,
           class In2V, class Out2V, int BLOCK, int ITEMS, class CT = unsigned long long>
-__global__ void __launch_bounds__(BLOCK, 4) compact2_kernel(InV in, StV stencil, Pred pred, ValT value, OutV out,
+__global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV in, StV stencil, Pred pred, ValT value, OutV out,
                                                          FalseV out_false, In2V in2, Out2V out2, size_t n,
                                                          size_t tiles, LookbackState st) {
     typedef typename remove_cvref<typename InV::value_t>::type E;
