@@ -409,3 +409,27 @@ def test_cuda_array_interface_vectors(trtc):
     y = torch.tensor([1.5, -2.0, 0.25], dtype=torch.float64, device="cuda")
     w = trtc.DVNumbaVector(y)
     assert trtc.Reduce(w) == -0.25
+
+
+def test_inplace_compaction_large(trtc):
+    # in-place forms on contiguous vectors go through a pool temporary (two-phase kernel + copy
+    # back); a range of a vector takes the same route, a permuted view the one-pass kernel
+    rng = np.random.default_rng(41)
+    n = (3 << 20) + 11
+    x = rng.integers(0, 1000, n).astype(np.int32)
+    v = trtc.device_vector_from_numpy(x)
+    c = trtc.Remove_If(v, is_even(trtc))
+    assert c == int((x % 2 != 0).sum()) and np.array_equal(v.to_host(0, c), x[x % 2 != 0])
+    y = np.repeat(rng.integers(0, 50, n // 4), 4)[: n - 100].astype(np.int32)
+    w = trtc.device_vector_from_numpy(np.concatenate([np.zeros(100, np.int32), y]))
+    c = trtc.Unique(w.range(100, 100 + len(y)), trtc.EqualTo())
+    keep = np.concatenate([[True], y[1:] != y[:-1]])
+    got = w.to_host(100, 100 + c)
+    assert c == int(keep.sum()) and np.array_equal(got, y[keep])
+    assert np.array_equal(w.to_host(0, 100), np.zeros(100, np.int32))  # outside the range: untouched
+    z = np.arange(20000, dtype=np.int32)
+    base = trtc.device_vector_from_numpy(z)
+    rev = trtc.DVReverse(base)
+    c = trtc.Remove_If(rev, is_even(trtc))  # reversed view: elements 19999, 19997, ... kept in order
+    out = base.to_host()
+    assert c == 10000 and np.array_equal(out[::-1][:c], z[::-1][z[::-1] % 2 != 0])
