@@ -73,3 +73,38 @@ def test_cuda_array_interface_adaptor_checks_dtype_and_contiguity():
         t.DVCupyVector(Fake("<f2", (4,)))          # float16: no element type of the library
     with pytest.raises(ValueError):
         t.DVNumbaVector(Fake("<i4", (4,), (8,)))   # strided
+
+
+def test_cpp_api_links_against_the_library(tmp_path):
+    # every TRTC_* declaration of include/thrustrtc_cpp.h (the C++ API the reference's JNI and
+    # C++/CLI shims call) resolves, with its declared signature, in libPyThrustRTC.so
+    import re
+    import shutil
+    import subprocess
+    if not shutil.which("g++"):
+        pytest.skip("no C++ compiler")
+    inc = os.path.join(ROOT, "include")
+    src = open(os.path.join(inc, "thrustrtc_cpp.h")).read()
+    decls = re.findall(r"THRUST_RTC_API\s+([\w:<>\*&\s]+?)\s+(TRTC_\w+)\s*\(([^;{]*?)\)\s*;", src, re.S)
+    assert len(decls) > 100
+    lines = []
+    for ret, name, params in decls:
+        params = " ".join(params.split())
+        types = []
+        if params and params != "void":
+            for p in params.split(","):
+                p = re.sub(r"\s*=.*$", "", p.strip())
+                types.append(re.sub(r"\s*\b\w+$", "", p))
+        lines.append("    f.push_back(reinterpret_cast<void (*)()>(static_cast<%s (*)(%s)>(&%s)));"
+                     % (" ".join(ret.split()), ", ".join(types), name))
+    cpp = tmp_path / "api_link.cpp"
+    cpp.write_text('#include "thrustrtc_cpp.h"\n#include <cstdio>\n#include <vector>\nint main() {\n'
+                   "    std::vector<void (*)()> f;\n" + "\n".join(lines) +
+                   '\n    std::printf("%zu\\n", f.size());\n    return 0;\n}\n')
+    exe = tmp_path / "api_link"
+    lib_dir = os.path.join(ROOT, "thrustrtc_b200")
+    r = subprocess.run(["g++", "-std=c++17", "-I", inc, str(cpp), "-o", str(exe), "-L", lib_dir, "-lPyThrustRTC",
+                        "-Wl,-rpath," + lib_dir], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and int(r.stdout.strip()) == len(decls), r.stderr
