@@ -10,6 +10,8 @@ reference tree; the fixtures themselves are committed and read by the tests).
   (and values 10000-i for the by-key case).
 * builtin_h_probe.json -- d_u32/d_u64 and Maximum/Minimum evaluated by the reference's own
   built_in.h compiled on the CPU (oracle/build_ref_probe.py).
+* api_h_exports.json -- the names of the reference's exported C functions
+  (python/api.h), which the drop-in library must export too.
 """
 import ctypes
 import json
@@ -58,7 +60,20 @@ def glibc_shuffles():
     return a, keys, vals
 
 
+REF_ROOT = os.environ.get("TRTC_REFERENCE_ROOT", "/root/reference")
+
+
+def api_h_exports():
+    import re
+    text = open(os.path.join(REF_ROOT, "python", "api.h")).read()
+    names = sorted(set(re.findall(r"PY_THRUSTRTC_API\s+[\w\s\*]+?\b(n_\w+)\s*\(", text)))
+    return {"source": "python/api.h", "names": names}
+
+
 def main():
+    if os.path.isdir(REF_ROOT):
+        with open(os.path.join(HERE, "api_h_exports.json"), "w") as f:
+            json.dump(api_h_exports(), f, indent=1)
     with open(os.path.join(HERE, "docs_vectors.json"), "w") as f:
         json.dump(DOCS, f, indent=1)
     a, k, v = glibc_shuffles()

@@ -108,3 +108,14 @@ def test_cpp_api_links_against_the_library(tmp_path):
     assert r.returncode == 0, r.stderr[-3000:]
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and int(r.stdout.strip()) == len(decls), r.stderr
+
+
+def test_every_reference_export_is_present():
+    # the reference's python/api.h exports (tests/golden/api_h_exports.json, written by
+    # tests/golden/make_golden.py from the reference tree) all resolve in this library
+    import json
+    names = json.load(open(os.path.join(ROOT, "tests", "golden", "api_h_exports.json")))["names"]
+    assert len(names) > 140
+    lib = ctypes.CDLL(LIB)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert missing == []
