@@ -347,3 +347,66 @@ def test_merge(trtc):
         ko, vo = trtc.device_vector("int32_t", na + nb), trtc.device_vector("int32_t", na + nb)
         trtc.Merge_By_Key(dv(x), dv(y), dv(vx), dv(vy), ko, vo)
         assert np.array_equal(ko.to_host(), ek) and np.array_equal(vo.to_host(), ev)
+
+
+def test_fake_vector_programs(trtc):
+    # python/test/test_constant.py, test_counter.py, test_discard.py, test_permutation.py,
+    # test_range.py, test_reverse.py, test_transform_iter.py with their printed values asserted
+    d = trtc.device_vector_from_list([3, 7, 2, 5], "int32_t")
+    trtc.Transform_Binary(d, trtc.DVConstant(trtc.DVInt32(10)), d, trtc.Plus())
+    assert host(d) == [13, 17, 12, 15]
+    d = trtc.device_vector("int32_t", 10)
+    trtc.Transform(trtc.DVCounter(trtc.DVInt32(5), 10), d, trtc.Negate())
+    assert host(d) == [-5 - i for i in range(10)]
+    trtc.Transform(trtc.DVCounter(trtc.DVInt32(5), 10), trtc.DVDiscard("int32_t"), trtc.Negate())  # no effect, no error
+    vals = trtc.device_vector_from_list([10.0, 20.0, 30.0, 40.0, 50.0, 60.0, 70.0, 80.0], "float")
+    idx = trtc.device_vector_from_list([2, 6, 1, 3], "int32_t")
+    out = trtc.device_vector("float", 4)
+    trtc.Transform(trtc.DVPermutation(vals, idx), out, trtc.Negate())
+    assert host(out) == [-30.0, -70.0, -20.0, -40.0]
+    din = trtc.device_vector_from_list([10, 20, 30, 40, 50, 60, 70, 80], "int32_t")
+    dout = trtc.device_vector("int32_t", 4)
+    trtc.Copy(din.range(2, 6), dout)
+    assert host(dout) == [30, 40, 50, 60]
+    din = trtc.device_vector_from_list([3, 7, 2, 5], "int32_t")
+    trtc.Transform(trtc.DVReverse(din), dout, trtc.Negate())
+    assert host(dout) == [-5, -2, -7, -3]
+    sq = trtc.Functor({}, ["x"], "\n         return sqrtf(x);\n")
+    f = trtc.device_vector_from_list([1.0, 4.0, 9.0, 16.0], "float")
+    fo = trtc.device_vector("float", 4)
+    trtc.Transform(trtc.DVTransform(f, "float", sq), fo, trtc.Negate())
+    assert host(fo) == [-1.0, -2.0, -3.0, -4.0]
+
+
+def test_multithread_program(trtc):
+    # python/test/test_multithread.py: one For kernel launched from three host threads at once
+    import threading
+    darr = trtc.device_vector_from_numpy(np.array([1.0, 2.0, 3.0, 4.0, 5.0], dtype=np.float32))
+    loop = trtc.For(["arr_in", "arr_out", "k"], "idx", "\n\tarr_out[idx] = arr_in[idx]*k;\n\t")
+    results, errors = [], []
+
+    def work():
+        try:
+            o = trtc.device_vector("float", 5)
+            loop.launch_n(5, [darr, o, trtc.DVFloat(10.0)])
+            results.append(o.to_host().tolist())
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    ts = [threading.Thread(target=work) for _ in range(3)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errors and results == [[10.0, 20.0, 30.0, 40.0, 50.0]] * 3
+
+
+def test_fft_program_fill(trtc):
+    # python/test/test_fft.py: Fill of a complex64 device array adapted through the CUDA Array
+    # Interface, then a library FFT of it (torch here in place of CuPy)
+    import torch
+    arr = torch.empty(4, dtype=torch.complex64, device="cuda")
+    trtc.Fill(trtc.DVCupyVector(arr), trtc.DVComplex64(complex(1.0, 2.0)))
+    torch.cuda.synchronize()
+    assert arr.cpu().tolist() == [complex(1.0, 2.0)] * 4
+    assert torch.fft.fft(arr).cpu().tolist() == [complex(4.0, 8.0), 0j, 0j, 0j]
