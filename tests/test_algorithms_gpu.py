@@ -410,3 +410,38 @@ def test_fft_program_fill(trtc):
     torch.cuda.synchronize()
     assert arr.cpu().tolist() == [complex(1.0, 2.0)] * 4
     assert torch.fft.fft(arr).cpu().tolist() == [complex(4.0, 8.0), 0j, 0j, 0j]
+
+
+def test_kernel_program_two_types(trtc):
+    # python/test/test_trtc.py: one Kernel launched with float and with int32 arguments
+    harr = np.array([1.0, 2.0, 3.0, 4.0, 5.0], dtype=np.float32)
+    darr = trtc.device_vector_from_numpy(harr)
+    assert darr.name_view_cls() == "VectorView<float>"
+    darr2 = trtc.device_vector_from_numpy(np.array([6, 7, 8, 9, 10], dtype=np.int32))
+    kernel = trtc.Kernel(["arr_in", "arr_out", "k"], """
+    size_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= arr_in.size()) return;
+    arr_out[idx] = arr_in[idx]*k;
+    """)
+    out = trtc.device_vector("float", 5)
+    kernel.launch(1, 128, [darr, out, trtc.DVFloat(10.0)])
+    assert host(out) == [10.0, 20.0, 30.0, 40.0, 50.0]
+    out = trtc.device_vector("int32_t", 5)
+    kernel.launch(1, 128, [darr2, out, trtc.DVInt32(5)])
+    assert host(out) == [30, 35, 40, 45, 50]
+
+
+def test_custom_vector_reduce_by_key_program(trtc):
+    # python/test/test_custom_vector.py: keys and values computed on the fly, keys discarded
+    darr = trtc.device_vector("int32_t", 2000)
+    trtc.Sequence(darr)
+    vals = trtc.DVCustomVector({"src": darr}, "idx", """
+    unsigned group = idx / src.size();
+    unsigned sub_idx = idx % src.size();
+    return src[sub_idx] % (group+1) ==0 ? 1: 0;
+""", "uint32_t", 20000)
+    keys = trtc.DVCustomVector({"src": darr}, "idx", "\n\treturn idx / src.size();\n", "uint32_t", 20000)
+    out = trtc.device_vector("uint32_t", 10)
+    c = trtc.Reduce_By_Key(keys, vals, trtc.DVDiscard("uint32_t", 10), out)
+    assert c == 10
+    assert host(out) == [sum(1 for x in range(2000) if x % (g + 1) == 0) for g in range(10)]
