@@ -433,3 +433,28 @@ def test_inplace_compaction_large(trtc):
     c = trtc.Remove_If(rev, is_even(trtc))  # reversed view: elements 19999, 19997, ... kept in order
     out = base.to_host()
     assert c == 10000 and np.array_equal(out[::-1][:c], z[::-1][z[::-1] % 2 != 0])
+
+
+def test_vector_storage_reused_and_bounded(trtc):
+    # DVVector storage comes from a pool of its own: a destroyed vector's memory serves the
+    # next vector without a new mapping, and beyond 8 GiB of cached storage it goes back to
+    # the device at the next synchronisation (as cudaFree would have returned it)
+    import gc
+    import torch
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    big = trtc.device_vector("int8_t", 24 << 30)
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 >= (16 << 30)  # storage cached by earlier tests' vectors may serve a part
+    assert trtc.Count(big.range(0, 1 << 20), trtc.DVInt8(0)) == 1 << 20  # zero-filled
+    del big
+    gc.collect()
+    torch.cuda.synchronize()
+    free2 = torch.cuda.mem_get_info()[0]
+    assert free2 - free1 >= (16 << 30) - (64 << 20)  # all but the 8 GiB cache went back
+    assert free0 - free2 <= (8 << 30) + (64 << 20)
+    x = np.arange(1 << 20, dtype=np.int32)
+    for _ in range(3):  # create / destroy cycles keep their contents right
+        v = trtc.device_vector_from_numpy(x)
+        assert np.array_equal(v.to_host(), x)
+        del v

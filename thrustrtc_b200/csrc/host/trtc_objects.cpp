@@ -101,13 +101,13 @@ DVVector::DVVector(const char* elem_cls, size_t size, void* hdata)
     if (!ensure_device()) return;
     const size_t bytes = m_elem_size * m_size;
     if (bytes == 0) return;
-    if (!TRTC_CUDA(cudaMalloc(&m_data, bytes))) { m_data = nullptr; return; }
+    if (!(m_data = vector_alloc(bytes))) return;
     if (hdata) TRTC_CUDA(cudaMemcpy(m_data, hdata, bytes, cudaMemcpyHostToDevice));
     else TRTC_CUDA(cudaMemset(m_data, 0, bytes));
 }
 
 DVVector::~DVVector() {
-    if (m_data) cudaFree(m_data);
+    vector_free(m_data);
 }
 
 void DVVector::to_host(void* hdata, size_t begin, size_t end) const {

@@ -106,6 +106,10 @@ static bool g_init_ok = false;
 static uint32_t* g_err_host = nullptr;
 static uint32_t* g_err_dev = nullptr;
 static int g_sms = 0;
+static cudaMemPool_t g_vec_pool = nullptr;
+// freed DVVector storage kept mapped for the next vectors; above this the pool gives memory
+// back to the device at the next synchronisation
+static const uint64_t kVectorCacheBytes = 8ull << 30;
 
 bool ensure_device() {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -128,6 +132,19 @@ bool ensure_device() {
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
         uint64_t thr = ~0ull;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    // DVVector storage: a pool of its own, so that creating and destroying vectors reuses
+    // mapped memory instead of mapping and unmapping device pages in cudaMalloc / cudaFree
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if (cudaMemPoolCreate(&g_vec_pool, &props) == cudaSuccess) {
+        uint64_t thr = kVectorCacheBytes;
+        cudaMemPoolSetAttribute(g_vec_pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    } else {
+        cudaGetLastError();
+        g_vec_pool = nullptr;
     }
     g_init_ok = true;
     return true;
@@ -238,6 +255,34 @@ void* tmp_alloc(size_t bytes, cudaStream_t s) {
 }
 void tmp_free(void* p, cudaStream_t s) {
     if (p) cudaFreeAsync(p, s);
+}
+
+void* vector_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (!g_vec_pool) return TRTC_CUDA(cudaMalloc(&p, bytes)) ? p : nullptr;
+    // ordered on the legacy default stream, like the copy or memset that fills the vector
+    if (cudaMallocFromPoolAsync(&p, bytes, g_vec_pool, 0) == cudaSuccess) return p;
+    cudaGetLastError();
+    // out of memory: give the cached blocks of both pools back to the device, then retry once
+    cudaDeviceSynchronize();
+    int dev = 0;
+    cudaMemPool_t def;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&def, dev) == cudaSuccess)
+        cudaMemPoolTrimTo(def, 0);
+    cudaMemPoolTrimTo(g_vec_pool, 0);
+    p = nullptr;
+    return TRTC_CUDA(cudaMallocFromPoolAsync(&p, bytes, g_vec_pool, 0)) ? p : nullptr;
+}
+void vector_free(void* p) {
+    if (!p) return;
+    if (!g_vec_pool) {
+        cudaFree(p);
+        return;
+    }
+    // cudaFree waits for all work on the device before the memory can be reused; keep that
+    // for work on other streams that may still read the vector
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, 0);
 }
 
 }  // namespace trtc_host

@@ -68,6 +68,10 @@ void* sort_ctrl_ws(cudaStream_t s, size_t bytes);
 // stream-ordered temporaries (cached by the CUDA memory pool)
 void* tmp_alloc(size_t bytes, cudaStream_t s);
 void tmp_free(void* p, cudaStream_t s);
+// DVVector storage (a pool of its own that keeps up to 8 GiB of freed vectors mapped);
+// vector_free waits for the device like cudaFree
+void* vector_alloc(size_t bytes);
+void vector_free(void* p);
 
 int sm_count();
 
