@@ -867,17 +867,25 @@ __global__ void __launch_bounds__(BLOCK) scan_by_key_kernel(KV keys, InV vals, O
 // phase 1 reads a tile (16-byte loads of keys and values) and publishes its segmented
 // aggregate -- the sum after its last segment head, with a head flag -- phase 2 looks back
 // (segmented: the walk stops at the first tile holding a head), re-reads the tile (normally
-// from L2) and writes it.  No tile data is held in registers across a wait.  Elements past
-// n (last tile) or every element of unaligned arrays take scalar loads; elements past n
-// count as heads of value T() and are not stored, so they never reach a valid output.
+// from L2) and writes it.  No tile data is held in registers across a wait.  A full warp
+// segment of aligned arrays is scanned in blocked order (each lane ITEMS consecutive
+// elements, re-laid out through shared memory); the rest of the last tile, and every element
+// of unaligned arrays, is scanned row by row with scalar loads; elements past n count as
+// heads of value T() and are not stored, so they never reach a valid output.
 #ifndef TRTC_SBK2_AHEAD
 #define TRTC_SBK2_AHEAD 0  // draw the next tile's ticket during the look-back instead of after
 #endif
-#ifndef TRTC_SBK2_MINB
-#define TRTC_SBK2_MINB 4  // resident CTAs per SM the kernel is compiled for
+#ifndef TRTC_SBK2_MINB  // resident CTAs per SM the kernel is compiled for (48 registers at 5)
+#define TRTC_SBK2_MINB(bytes) ((bytes) == 8 ? 4 : 5)
+#endif
+// full aligned warp segments are re-laid out through shared memory so that each lane holds
+// ITEMS consecutive elements: one warp-wide segmented scan per segment instead of one per
+// 16-byte row
+#ifndef TRTC_SBK2_BLOCKED
+#define TRTC_SBK2_BLOCKED 1
 #endif
 template <class K, class T, int MODE, int BLOCK, int ITEMS>
-__global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __restrict__ keys, const T* vals, T* out,
+__global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB(sizeof(T))) sbk2_kernel(const K* __restrict__ keys, const T* vals, T* out,
                                                                      size_t n, size_t tiles, T init, LookbackState st) {
     static_assert(sizeof(K) == sizeof(T) && (sizeof(T) == 4 || sizeof(T) == 8), "keys and values of one width");
     constexpr int VEC = VecWidth<T>::V;
@@ -897,6 +905,9 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
     __shared__ int s_agg_hd[2];
     __shared__ T s_pre;
     __shared__ int s_pre_h;
+    constexpr int SB = TRTC_SBK2_BLOCKED ? WARPS * WSEG : VEC;
+    __shared__ __align__(16) K s_bk[SB];  // per-warp staging of the blocked re-layout
+    __shared__ __align__(16) T s_bv[SB];
     Plus op;
     EqualTo eq;
 
@@ -949,44 +960,107 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
         if (i0 == 0) hd[0] = true;
     };
     auto first_key = [&](size_t wstart) -> K { return wstart > 0 && wstart - 1 < n ? keys[wstart - 1] : K(); };
+    // a full aligned warp segment in blocked order: lane l receives elements
+    // wstart + l*ITEMS .. + ITEMS-1 (16-byte row loads, staged in shared memory: row r, lane l
+    // writes 16-byte slot r*32+l; lane l reads slots l*ROWS .. l*ROWS+ROWS-1).  Returns the
+    // lane's head mask (bit j: element j starts a segment).
+    auto load_blocked = [&](size_t wstart, bool phase2, K (&k)[ITEMS], T (&x)[ITEMS]) -> uint32_t {
+        static_assert(ITEMS <= 32, "head mask");
+        VecK kq[ROWS];
+        VecT vq[ROWS];
+        preload(wstart, phase2, kq, vq);
+        uint4* sk4 = reinterpret_cast<uint4*>(s_bk + warp * WSEG);
+        uint4* sv4 = reinterpret_cast<uint4*>(s_bv + warp * WSEG);
+#pragma unroll
+        for (int r = 0; r < ROWS; r++) {
+            sk4[r * 32 + lane] = kq[r].q;
+            sv4[r * 32 + lane] = vq[r].q;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < ROWS; q++) {
+            VecK a;
+            VecT b;
+            a.q = sk4[lane * ROWS + q];
+            b.q = sv4[lane * ROWS + q];
+#pragma unroll
+            for (int e = 0; e < VEC; e++) {
+                k[q * VEC + e] = a.k[e];
+                x[q * VEC + e] = b.t[e];
+            }
+        }
+        K pk = shfl_up_any(k[ITEMS - 1], 1);
+        if (lane == 0) pk = first_key(wstart);
+        uint32_t hd = 0;
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const K before = j == 0 ? pk : k[j - 1];
+            if (!(bool)eq(before, k[j])) hd |= 1u << j;
+        }
+        if (wstart == 0 && lane == 0) hd |= 1u;
+        return hd;
+    };
+    // the lane's value after its last head (all its elements when it holds none)
+    auto lane_fold = [&](const T (&x)[ITEMS], uint32_t hd) -> T {
+        T a = x[0];
+#pragma unroll
+        for (int j = 1; j < ITEMS; j++) a = ((hd >> j) & 1u) ? x[j] : (T)op(a, x[j]);
+        return a;
+    };
 
     // ---- phase 1: segmented warp aggregates (ordered), tile aggregate, publication
     auto phase1 = [&](size_t tile, int b) {
         const size_t wstart = tile * (size_t)TILE + (size_t)warp * WSEG;
         const bool fast = aligned && wstart + WSEG <= n;
-        K prevk = first_key(wstart);
         T wt = T();
         bool wt_h = false, wt_hd = false;
-        VecK kq[ROWS];
-        VecT vq[ROWS];
-        if (fast) preload(wstart, false, kq, vq);
-#pragma unroll
-        for (int r = 0; r < ROWS; r++) {
-            K k[VEC];
-            T x[VEC];
-            bool hd[VEC];
-            load_row(wstart, r, fast, prevk, kq[r], vq[r], k, x, hd);
-            prevk = shfl_any(k[VEC - 1], 31);
-            // lane fold (value after the lane's last head)
-            T a = x[0];
-            bool ahd = hd[0];
-#pragma unroll
-            for (int e = 1; e < VEC; e++) {
-                if (hd[e]) { a = x[e]; ahd = true; }
-                else a = (T)op(a, x[e]);
-            }
-            // the row's value after its last head: the lanes from the last lane holding a
-            // head (lane 0 when none) summed by a butterfly (Plus, T() its identity)
-            const uint32_t hm = __ballot_sync(0xffffffffu, ahd);
+        if (TRTC_SBK2_BLOCKED && fast) {
+            K k[ITEMS];
+            T x[ITEMS];
+            const uint32_t hd = load_blocked(wstart, false, k, x);
+            T a = lane_fold(x, hd);
+            // the segment's value after its last head: lanes from the last lane holding a head
+            // (lane 0 when none) summed by a butterfly
+            const uint32_t hm = __ballot_sync(0xffffffffu, hd != 0u);
             const uint32_t last = hm ? 31u - __clz(hm) : 0u;
             a = lane >= last ? a : T();
 #pragma unroll
             for (int d = 16; d > 0; d >>= 1) a = (T)op(a, shfl_xor_any(a, d));
-            ahd = hm != 0;
-            if (!wt_h || ahd) wt = a;
-            else wt = (T)op(wt, a);
-            wt_h = true;
-            wt_hd = wt_hd || ahd;
+            wt = a;
+            wt_hd = hm != 0u;
+        } else {
+            K prevk = first_key(wstart);
+            VecK kq[ROWS];
+            VecT vq[ROWS];
+            if (fast) preload(wstart, false, kq, vq);
+#pragma unroll
+            for (int r = 0; r < ROWS; r++) {
+                K k[VEC];
+                T x[VEC];
+                bool hd[VEC];
+                load_row(wstart, r, fast, prevk, kq[r], vq[r], k, x, hd);
+                prevk = shfl_any(k[VEC - 1], 31);
+                // lane fold (value after the lane's last head)
+                T a = x[0];
+                bool ahd = hd[0];
+#pragma unroll
+                for (int e = 1; e < VEC; e++) {
+                    if (hd[e]) { a = x[e]; ahd = true; }
+                    else a = (T)op(a, x[e]);
+                }
+                // the row's value after its last head: the lanes from the last lane holding a
+                // head (lane 0 when none) summed by a butterfly (Plus, T() its identity)
+                const uint32_t hm = __ballot_sync(0xffffffffu, ahd);
+                const uint32_t last = hm ? 31u - __clz(hm) : 0u;
+                a = lane >= last ? a : T();
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) a = (T)op(a, shfl_xor_any(a, d));
+                ahd = hm != 0;
+                if (!wt_h || ahd) wt = a;
+                else wt = (T)op(wt, a);
+                wt_h = true;
+                wt_hd = wt_hd || ahd;
+            }
         }
         if (lane == 0) { s_wtot[b][warp] = wt; s_whd[b][warp] = wt_hd ? 1 : 0; }
         __syncthreads();
@@ -1065,27 +1139,13 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
                 else carry = (T)op(carry, s_woff[buf][warp]);
                 carry_h = true;
             }
-            K prevk = first_key(wstart);
-            VecK kq[ROWS];
-            VecT vq[ROWS];
-            if (fast) preload(wstart, true, kq, vq);
-#pragma unroll
-            for (int r = 0; r < ROWS; r++) {
-                K k[VEC];
-                T x[VEC];
-                bool hd[VEC];
-                load_row(wstart, r, fast, prevk, kq[r], vq[r], k, x, hd);
-                prevk = shfl_any(k[VEC - 1], 31);
-                T a = x[0];
-                bool ahd = hd[0];
-#pragma unroll
-                for (int e = 1; e < VEC; e++) {
-                    if (hd[e]) { a = x[e]; ahd = true; }
-                    else a = (T)op(a, x[e]);
-                }
-                // inclusive segmented scan over the lanes: at distance d, lane l holds lanes
-                // (l-d, l] and takes in (l-2d, l-d] only if no lane of its window holds a head
-                const uint32_t hm = __ballot_sync(0xffffffffu, ahd);
+            if (TRTC_SBK2_BLOCKED && fast) {
+                K k[ITEMS];
+                T x[ITEMS];
+                const uint32_t hd = load_blocked(wstart, true, k, x);
+                const T a = lane_fold(x, hd);
+                // inclusive segmented scan over the lanes (as in the row form below)
+                const uint32_t hm = __ballot_sync(0xffffffffu, hd != 0u);
                 const uint32_t le = lane == 31u ? 0xffffffffu : ((2u << lane) - 1u);  // lanes <= l
                 T inc = a;
 #pragma unroll
@@ -1098,37 +1158,100 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB) sbk2_kernel(const K* __
                 }
                 const T ex = shfl_up_any(inc, 1);
                 const bool exhd = (hm & (le >> 1)) != 0u;  // a head in lanes < l
-                const T row_tot = shfl_any(inc, 31);
-                const bool row_hd = hm != 0u;
-                // running value entering this lane's first element
                 T run = carry;
                 bool run_h = carry_h;
                 if (lane > 0) {
                     run = (exhd || !run_h) ? ex : (T)op(run, ex);
                     run_h = true;
                 }
-                T y[VEC];
 #pragma unroll
-                for (int e = 0; e < VEC; e++) {
-                    const T c = hd[e] ? x[e] : (run_h ? (T)op(run, x[e]) : x[e]);
-                    if (MODE == 0) y[e] = c;
-                    else y[e] = hd[e] ? init : (T)op(init, run);
+                for (int j = 0; j < ITEMS; j++) {
+                    const bool h = (hd >> j) & 1u;
+                    const T c = h ? x[j] : (run_h ? (T)op(run, x[j]) : x[j]);
+                    const T y = MODE == 0 ? c : (h ? init : (T)op(init, run));
+                    x[j] = y;
                     run = c;
                     run_h = true;
                 }
-                const size_t i0 = wstart + (size_t)r * 32 * VEC + (size_t)lane * VEC;
-                if (fast) {
+                // back to rows through the lane's own staging slots, then 16-byte stores
+                uint4* sv4 = reinterpret_cast<uint4*>(s_bv + warp * WSEG);
+#pragma unroll
+                for (int q = 0; q < ROWS; q++) {
                     VecT o;
 #pragma unroll
-                    for (int e = 0; e < VEC; e++) o.t[e] = y[e];
-                    __stcs(reinterpret_cast<uint4*>(out + i0), o.q);
-                } else {
-#pragma unroll
-                    for (int e = 0; e < VEC; e++)
-                        if (i0 + e < n) out[i0 + e] = y[e];
+                    for (int e = 0; e < VEC; e++) o.t[e] = x[q * VEC + e];
+                    sv4[lane * ROWS + q] = o.q;
                 }
-                carry = (row_hd || !carry_h) ? row_tot : (T)op(carry, row_tot);
-                carry_h = true;
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < ROWS; r++)
+                    __stcs(reinterpret_cast<uint4*>(out + wstart + (size_t)(r * 32 + (int)lane) * VEC), sv4[r * 32 + lane]);
+            } else {
+                K prevk = first_key(wstart);
+                VecK kq[ROWS];
+                VecT vq[ROWS];
+                if (fast) preload(wstart, true, kq, vq);
+#pragma unroll
+                for (int r = 0; r < ROWS; r++) {
+                    K k[VEC];
+                    T x[VEC];
+                    bool hd[VEC];
+                    load_row(wstart, r, fast, prevk, kq[r], vq[r], k, x, hd);
+                    prevk = shfl_any(k[VEC - 1], 31);
+                    T a = x[0];
+                    bool ahd = hd[0];
+#pragma unroll
+                    for (int e = 1; e < VEC; e++) {
+                        if (hd[e]) { a = x[e]; ahd = true; }
+                        else a = (T)op(a, x[e]);
+                    }
+                    // inclusive segmented scan over the lanes: at distance d, lane l holds lanes
+                    // (l-d, l] and takes in (l-2d, l-d] only if no lane of its window holds a head
+                    const uint32_t hm = __ballot_sync(0xffffffffu, ahd);
+                    const uint32_t le = lane == 31u ? 0xffffffffu : ((2u << lane) - 1u);  // lanes <= l
+                    T inc = a;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const T y = shfl_up_any(inc, d);
+                        if (lane >= (uint32_t)d) {
+                            const uint32_t win = le & ~((1u << (lane - (uint32_t)d + 1u)) - 1u);
+                            if ((hm & win) == 0u) inc = (T)op(y, inc);
+                        }
+                    }
+                    const T ex = shfl_up_any(inc, 1);
+                    const bool exhd = (hm & (le >> 1)) != 0u;  // a head in lanes < l
+                    const T row_tot = shfl_any(inc, 31);
+                    const bool row_hd = hm != 0u;
+                    // running value entering this lane's first element
+                    T run = carry;
+                    bool run_h = carry_h;
+                    if (lane > 0) {
+                        run = (exhd || !run_h) ? ex : (T)op(run, ex);
+                        run_h = true;
+                    }
+                    T y[VEC];
+#pragma unroll
+                    for (int e = 0; e < VEC; e++) {
+                        const T c = hd[e] ? x[e] : (run_h ? (T)op(run, x[e]) : x[e]);
+                        if (MODE == 0) y[e] = c;
+                        else y[e] = hd[e] ? init : (T)op(init, run);
+                        run = c;
+                        run_h = true;
+                    }
+                    const size_t i0 = wstart + (size_t)r * 32 * VEC + (size_t)lane * VEC;
+                    if (fast) {
+                        VecT o;
+#pragma unroll
+                        for (int e = 0; e < VEC; e++) o.t[e] = y[e];
+                        __stcs(reinterpret_cast<uint4*>(out + i0), o.q);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < VEC; e++)
+                            if (i0 + e < n) out[i0 + e] = y[e];
+                    }
+                    carry = (row_hd || !carry_h) ? row_tot : (T)op(carry, row_tot);
+                    carry_h = true;
+                }
             }
         }
         if (nxt >= tiles) break;

@@ -164,9 +164,11 @@ bool reduce_raw(int tc, int op, const void* in, size_t n, const void* init, void
 #ifndef TRTC_SBK2
 #define TRTC_SBK2 1  // two-phase segmented scan for keys and values of one width
 #endif
-// B200, 2^28 i32 keys / f32 values in runs of ~32: 8 items at 2 / 5 CTAs per SM 1.36 / 0.99 ms,
-// 12 items at 4 CTAs 0.93 ms, 16 items at 3 CTAs 1.06 ms; drawing the next ticket during the
-// look-back (TRTC_SBK2_AHEAD) 0.95 ms at 8 and 12 items
+// B200, 2^28 i32 keys / f32 values in runs of ~32.  Row form: 8 items at 2 / 5 CTAs per SM
+// 1.36 / 0.99 ms, 12 items at 4 CTAs 0.93 ms, 16 items at 3 CTAs 1.06 ms.  Blocked form
+// (TRTC_SBK2_BLOCKED): 12 items at 4 / 5 / 6 CTAs 0.87 / 0.80 / 0.87 ms, 16 items at 4 CTAs
+// 1.14 ms, 8 items at 6 / 8 CTAs 0.98 / 0.93 ms.  Drawing the next ticket during the
+// look-back (TRTC_SBK2_AHEAD) gained nothing in either form.
 #ifndef TRTC_SBK2_ITEMS
 #define TRTC_SBK2_ITEMS 12  // elements per thread of a two-phase segmented-scan tile (4-byte types)
 #endif
