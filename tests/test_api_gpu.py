@@ -458,3 +458,16 @@ def test_vector_storage_reused_and_bounded(trtc):
         v = trtc.device_vector_from_numpy(x)
         assert np.array_equal(v.to_host(), x)
         del v
+
+
+def test_vector_pool_can_be_switched_off(cuda):
+    # TRTC_VECTOR_POOL=0 (read once, at device initialisation) keeps one cudaMalloc per vector
+    import subprocess
+    import sys
+    code = ("import numpy as np, thrustrtc_b200 as t; t.init(); x = np.arange(1000, dtype=np.int32); "
+            "v = t.device_vector_from_numpy(x); assert np.array_equal(v.to_host(), x); "
+            "t.Sort(v); assert t.Reduce(v) == int(x.sum()); del v; print('ok')")
+    env = dict(os.environ, TRTC_VECTOR_POOL="0")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]

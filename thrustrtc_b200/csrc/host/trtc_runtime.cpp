@@ -3,9 +3,11 @@
 
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 namespace trtc_host {
@@ -135,11 +137,15 @@ bool ensure_device() {
     }
     // DVVector storage: a pool of its own, so that creating and destroying vectors reuses
     // mapped memory instead of mapping and unmapping device pages in cudaMalloc / cudaFree
+    // (TRTC_VECTOR_POOL=0 keeps one cudaMalloc per vector, e.g. for CUDA IPC export)
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
     props.location.id = dev;
-    if (cudaMemPoolCreate(&g_vec_pool, &props) == cudaSuccess) {
+    const char* vp = getenv("TRTC_VECTOR_POOL");
+    if (vp && std::string(vp) == "0") {
+        g_vec_pool = nullptr;
+    } else if (cudaMemPoolCreate(&g_vec_pool, &props) == cudaSuccess) {
         uint64_t thr = kVectorCacheBytes;
         cudaMemPoolSetAttribute(g_vec_pool, cudaMemPoolAttrReleaseThreshold, &thr);
     } else {
