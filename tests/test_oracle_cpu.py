@@ -139,3 +139,38 @@ def test_remaining_algorithm_restatements():
     assert not O.is_partitioned(np.arange(1, 11) % 2 == 0)
     assert O.adjacent_difference(np.array([1, 2, 1, 2, 1, 2, 1, 2], np.int32)).tolist() == [1, 1, -1, 1, -1, 1, -1, 1]
     assert O.first_true([False, False]) is None and O.first_true([0, 1, 1]) == 1
+
+
+def test_reference_hot_path_programs_hand_worked():
+    # the inputs of python/test/test_scan.py, test_transform_scan.py, test_scan_by_key.py,
+    # test_remove.py, test_sort.py and test_unique.py, with their printed values worked by
+    # hand from Thrust's semantics (the programs print without expected outputs)
+    i32 = lambda v: np.array(v, np.int32)
+    a, m = i32([1, 0, 2, 2, 1, 3]), i32([-5, 0, 2, -3, 2, 4, 0, -1, 2, 8])
+    assert O.scan(a).tolist() == [1, 1, 3, 5, 6, 9]
+    assert O.scan(m, "Maximum").tolist() == [-5, 0, 2, 2, 2, 4, 4, 4, 4, 8]
+    assert O.scan(a, exclusive=True).tolist() == [0, 1, 1, 3, 5, 6]
+    assert O.scan(a, exclusive=True, init=4).tolist() == [4, 5, 5, 7, 9, 10]
+    assert O.scan(m, "Maximum", True, 1).tolist() == [1, 1, 1, 2, 2, 2, 4, 4, 4, 4]
+    assert O.scan(-a).tolist() == [-1, -1, -3, -5, -6, -9]
+    assert O.scan(-a, exclusive=True, init=4).tolist() == [4, 3, 3, 1, -1, -2]
+    k, ones = i32([0, 0, 0, 1, 1, 2, 3, 3, 3, 3]), i32([1] * 10)
+    assert O.scan_by_key(k, ones).tolist() == [1, 2, 3, 1, 2, 1, 1, 2, 3, 4]
+    assert O.scan_by_key(k, ones, exclusive=True).tolist() == [0, 1, 2, 0, 1, 0, 0, 1, 2, 3]
+    assert O.scan_by_key(k, ones, exclusive=True, init=5).tolist() == [5, 6, 7, 5, 6, 5, 5, 6, 7, 8]
+    x = i32([3, 1, 4, 1, 5, 9])
+    assert x[O.remove_flags(x, 1)].tolist() == [3, 4, 5, 9]
+    y = i32([-2, 0, -1, 0, 1, 2])
+    assert y[O.remove_flags(y, 0)].tolist() == [-2, -1, 1, 2]
+    assert O.copy_if(y, y % 2 != 0).tolist() == [-1, 1]
+    z = i32([1, 4, 2, 8, 5, 7])
+    assert O.copy_if(z, z % 2 != 0).tolist() == [1, 5, 7]
+    assert O.copy_if(z, i32([0, 1, 1, 1, 0, 0]) == 0).tolist() == [1, 5, 7]
+    assert O.sort(z).tolist() == [1, 2, 4, 5, 7, 8] and O.sort(z, True).tolist() == [8, 7, 5, 4, 2, 1]
+    sk, sv = O.sort_by_key(z, i32([1, 2, 3, 4, 5, 6]))
+    assert sk.tolist() == [1, 2, 4, 5, 7, 8] and sv.tolist() == [1, 3, 2, 5, 6, 4]
+    sk, sv = O.sort_by_key(z, i32([1, 2, 3, 4, 5, 6]), True)
+    assert sk.tolist() == [8, 7, 5, 4, 2, 1] and sv.tolist() == [4, 6, 5, 2, 3, 1]
+    u, uv = i32([1, 3, 3, 3, 2, 2, 1]), i32([9, 8, 7, 6, 5, 4, 3])
+    f = O.unique_flags(u)
+    assert u[f].tolist() == [1, 3, 2, 1] and uv[f].tolist() == [9, 8, 5, 3]
