@@ -4,7 +4,11 @@
 Default workload: stable Sort_By_Key of 2^28 uint32 keys (uniform over the 32-bit range,
 SplitMix64 seed 0) with uint32 values = index, ascending -- the reference's headline case.
 Other workloads (--workload): inclusive scan of 2^28 int32 in [-1000, 1000], reduce of 2^28
-float32 in [0, 1).
+float32 in [0, 1); the mixed-type cases c1_sort_by_key_2e20, c3a_sort_f32,
+c3b_sort_by_key_i64_zipf, c3c_copy_if_functor and c3d_scan_by_key_f32; the batched form
+segmented_c4 (100,000 lognormal segments sorted and scanned in one launch, beside one plain
+call pair per segment); and serving_c5 (the request server against one plain call per
+request).
 
 One JSON line on rank 0:
   value        whole-job throughput with inputs resident in HBM (device-timed with CUDA
