@@ -174,3 +174,24 @@ def test_reference_hot_path_programs_hand_worked():
     u, uv = i32([1, 3, 3, 3, 2, 2, 1]), i32([9, 8, 7, 6, 5, 4, 3])
     f = O.unique_flags(u)
     assert u[f].tolist() == [1, 3, 2, 1] and uv[f].tolist() == [9, 8, 5, 3]
+
+
+@pytest.mark.parametrize("dt", [np.uint32, np.int32, np.float32])
+def test_threaded_pair_sort_equals_the_oracle_order(dt):
+    # the timed host baseline (packed key'|index words, parallel chunks, pairwise merges)
+    # must produce exactly sort_by_key's order, whatever the thread count
+    rng = np.random.default_rng(21)
+    n = 100_003
+    if dt == np.float32:
+        x = rng.standard_normal(n).astype(dt)
+        x[rng.integers(0, n, 500)] = -0.0
+        x[rng.integers(0, n, 50)] = np.nan
+        x[rng.integers(0, n, 2000)] = x[rng.integers(0, n, 2000)]
+    else:
+        x = rng.integers(0, 5000, n).astype(dt)  # many ties
+    v = np.arange(n, dtype=np.uint32)
+    for desc in (False, True):
+        ek, ev = O.sort_by_key(x, v, desc)
+        for threads in (1, 3, 4):
+            k, vv = O.sort_pairs32(x, v, desc, threads)
+            assert k.tobytes() == ek.tobytes() and vv.tobytes() == ev.tobytes(), (dt, desc, threads)
