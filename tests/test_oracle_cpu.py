@@ -195,3 +195,19 @@ def test_threaded_pair_sort_equals_the_oracle_order(dt):
         for threads in (1, 3, 4):
             k, vv = O.sort_pairs32(x, v, desc, threads)
             assert k.tobytes() == ek.tobytes() and vv.tobytes() == ev.tobytes(), (dt, desc, threads)
+
+
+def test_oracle_forms_agree_where_the_arithmetic_is_exact():
+    # integer-valued floats sum exactly in any order and width: the value-type scans, their
+    # FP64 forms, the sequential fold and the reference's 256-wide reduction tree must agree,
+    # and wrapping int32 sums must equal numpy's modulo-2^32 cumulative sums
+    rng = np.random.default_rng(5)
+    for n in (1, 255, 256, 257, 70_001):
+        f = rng.integers(0, 16, n).astype(np.float32)
+        assert O.scan(f).astype(np.float64).tolist() == O.scan_f64(f).tolist() == np.cumsum(f, dtype=np.float64).tolist()
+        assert float(O.reduce(f)) == O.reduce_f64(f) == float(O.reduce_tree(f)) == float(f.sum(dtype=np.float64))
+        k = np.repeat(np.arange(n), rng.integers(1, 5, n))[:n].astype(np.int32)
+        assert O.scan_by_key(k, f).astype(np.float64).tolist() == O.scan_by_key(k, f, f64=True).tolist()
+        i = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)
+        assert O.scan(i).tolist() == np.cumsum(i, dtype=np.int64).astype(np.int32).tolist()
+        assert O.reduce(i) == O.reduce_tree(i) == np.int32(np.int64(i.sum(dtype=np.int64)).astype(np.int32))
