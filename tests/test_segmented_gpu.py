@@ -153,3 +153,37 @@ def test_segmented_cuda_graph_replay(N):
         assert np.array_equal(tk.cpu().numpy().view(np.uint32), ek)
         assert np.array_equal(tv.cpu().numpy().view(np.uint32), ev)
         assert np.array_equal(ts.cpu().numpy().view(np.uint32), es)
+
+
+@pytest.mark.parametrize("desc", [False, True])
+def test_segmented_float_nan_rotation(N, desc):
+    # Segments holding NaNs get the reference's Min_Element rotation (extrema.cpp:5-13), as a
+    # Sort_By_Key call on the segment alone would: +NaN, -NaN, payload NaNs, NaN at the
+    # segment's index 0 (the tree then selects it), NaN only past the first 256-block, and
+    # segments of every class (one warp, on chip, global memory; > 65536 keys: three tree rounds).
+    rng = np.random.default_rng(41 + int(desc))
+    lens = np.array([1, 2, 5, 31, 33, 256, 257, 300, 513, 2047, 4096, 4097, 9000, 70000, 200, 1000, 3, 64],
+                    dtype=np.int64)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    n = int(off[-1])
+    keys = (rng.standard_normal(n) * 10).astype(np.float32)
+    keys[rng.integers(0, n, n // 40)] = -0.0
+    bits = keys.view(np.uint32)
+    pats = np.array([0x7FC00000, 0xFFC00000, 0x7FC00123, 0xFF800001], dtype=np.uint32)
+    for i in range(len(lens)):
+        a, b = off[i], off[i + 1]
+        mode = i % 4
+        if mode == 0:      # NaN at index 0 of the segment
+            bits[a] = pats[i % len(pats)]
+        elif mode == 1:    # NaNs scattered (may sit in left slots of the tree)
+            for j in rng.integers(a, b, max(1, (b - a) // 50)):
+                bits[j] = pats[int(j) % len(pats)]
+        elif mode == 2 and b - a > 300:  # NaN only after the first 256-block
+            bits[a + 280] = pats[1]
+        # mode 3: no NaN
+    vals = np.arange(n, dtype=np.uint32)
+    gk, gv, gs = run(N, "float", keys, vals, off, desc)
+    ek, ev, es = expected(keys, vals, off, desc)
+    assert gk.tobytes() == ek.tobytes()
+    assert np.array_equal(gv, ev)
+    assert np.array_equal(gs, es)

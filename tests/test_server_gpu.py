@@ -34,6 +34,18 @@ def L(cuda):
     return L
 
 
+NAN_BITS = np.array([0x7FC00000, 0xFFC00000, 0x7FC00123], dtype=np.uint32)
+
+
+def add_nans(rng, x):
+    """NaNs (+, -, payload) in a float sort request; at index 0 in a third of the requests
+    (the reference's Min_Element then selects the NaN and the sorted order is rotated)."""
+    b = x.view(np.uint32)
+    b[rng.integers(0, len(x), max(1, len(x) // 100))] = NAN_BITS[rng.integers(0, 3)]
+    if rng.random() < 0.34:
+        b[0] = NAN_BITS[rng.integers(0, 3)]
+
+
 def make_requests(rng, count, lo_log2, hi_log2):
     reqs = []
     for _ in range(count):
@@ -43,6 +55,8 @@ def make_requests(rng, count, lo_log2, hi_log2):
         dt = TYPES[t]
         if dt == np.float32:
             x = rng.standard_normal(n).astype(np.float32)
+            if kind == 0 and rng.random() < 0.5:
+                add_nans(rng, x)
         elif kind == 0:
             x = rng.integers(0, 1000, n).astype(dt)  # duplicates: stability matters
         else:
@@ -148,5 +162,54 @@ def test_server_admission_budget(L):
         drain(L, srv)
         for i, rid in enumerate(ids):
             check_oracle(0, reqs[i][2], run.result(srv, i, rid))
+    finally:
+        L.trtc_server_destroy(srv)
+
+
+def test_server_float_sorts_with_nan(L):
+    # coalesced (segmented kernel) and plain float Sort_By_Key requests holding NaNs give the
+    # order of the single-request call (the reference's Min_Element rotation included)
+    rng = np.random.default_rng(5)
+    reqs = []
+    for i in range(120):
+        n = int(2 ** rng.uniform(4, 14)) if i < 110 else int(2 ** rng.uniform(17, 19))
+        x = (rng.standard_normal(n) * 3).astype(np.float32)
+        add_nans(rng, x)
+        if i % 5 == 0:
+            x.view(np.uint32)[0] = NAN_BITS[i % 3]
+        reqs.append((0, 8, x))
+    srv = L.trtc_server_create(4 << 30, 4, 1 << 16)
+    assert srv
+    try:
+        run = Run(L, reqs)
+        ids = [run.submit(srv, i) for i in range(len(reqs))]
+        drain(L, srv)
+        for i, rid in enumerate(ids):
+            check_oracle(0, reqs[i][2], run.result(srv, i, rid))
+    finally:
+        L.trtc_server_destroy(srv)
+
+
+def test_server_refuses_request_beyond_budget(L):
+    # a request whose temporaries exceed the whole budget is refused at submission (-1 and a
+    # message), nothing of it runs, and the server keeps serving requests that fit
+    import torch
+    from thrustrtc_b200 import _native as N
+    srv = L.trtc_server_create(1 << 20, 2, 1 << 12)
+    assert srv
+    try:
+        big = torch.arange(1 << 20, dtype=torch.int32, device="cuda")
+        bigv = big.clone()
+        p = lambda a: ctypes.c_void_p(a.data_ptr())  # noqa: E731
+        assert L.trtc_server_submit(srv, 0, 5, p(big), p(bigv), None, 1 << 20) == -1
+        assert "budget" in N.last_error()
+        torch.cuda.synchronize()
+        assert torch.equal(big, bigv)
+        rng = np.random.default_rng(6)
+        reqs = [(0, 5, rng.integers(0, 2**32, 3000, dtype=np.uint64).astype(np.uint32))]
+        run = Run(L, reqs)
+        rid = run.submit(srv, 0)
+        drain(L, srv)
+        check_oracle(0, reqs[0][2], run.result(srv, 0, rid))
     finally:
         L.trtc_server_destroy(srv)

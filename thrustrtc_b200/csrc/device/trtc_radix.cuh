@@ -210,6 +210,36 @@ __global__ void __launch_bounds__(256) radix_plan_kernel(SortCtrl* ctrl, size_t 
 // a block the strided tree s = 128..1 with "if (tid < s && i + s < n) h[tid] = op(h[tid],
 // h[tid+s])", op(i1, i2) = v[i2] < v[i1] ? i2 : i1.  One warp handles one 256-block: lane l
 // holds slots l, l+32, ..., l+224.  FIRST: read keys; otherwise read a previous round.
+// One warp applies the tree to one 256-block of L <= 256 slots; load(t, v, i) yields slot t
+// (t < L).  Lane 0 holds the block's (value, index) on return.
+template <class K, class Load>
+TRTC_FORCEINLINE void min_tree_warp256(Load load, uint32_t L, K& out_v, unsigned long long& out_i) {
+    const uint32_t lane = threadIdx.x & 31u;
+    K v[8];
+    unsigned long long ix[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const uint32_t t = lane + 32u * k;
+        if (t < L) load(t, v[k], ix[k]);
+        else { v[k] = K(); ix[k] = 0; }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (lane + 32u * k + 128u < L && v[k + 4] < v[k]) { v[k] = v[k + 4]; ix[k] = ix[k + 4]; }
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+        if (lane + 32u * k + 64u < L && v[k + 2] < v[k]) { v[k] = v[k + 2]; ix[k] = ix[k + 2]; }
+    if (lane + 32u < L && v[1] < v[0]) { v[0] = v[1]; ix[0] = ix[1]; }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const K ov = shfl_down_any(v[0], s);
+        const unsigned long long oi = __shfl_down_sync(0xffffffffu, ix[0], s);
+        if (lane < (uint32_t)s && lane + s < L && ov < v[0]) { v[0] = ov; ix[0] = oi; }
+    }
+    out_v = v[0];
+    out_i = ix[0];
+}
+
 template <class K, bool FIRST, bool NAN_GATE>
 __global__ void __launch_bounds__(256) min_tree_kernel(const typename RadixKey<K>::B* __restrict__ keys,
                                                         const K* __restrict__ in_v,
@@ -223,32 +253,15 @@ __global__ void __launch_bounds__(256) min_tree_kernel(const typename RadixKey<K
     for (size_t b = (size_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); b < nb; b += warps_total) {
         const size_t base = b * 256;
         const uint32_t L = (uint32_t)((m - base) < 256 ? (m - base) : 256);
-        K v[8];
-        unsigned long long ix[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const uint32_t t = lane + 32u * k;
-            if (t < L) {
-                if (FIRST) { v[k] = RadixKey<K>::value(keys[base + t]); ix[k] = base + t; }
-                else { v[k] = in_v[base + t]; ix[k] = in_i[base + t]; }
-            } else {
-                v[k] = K(); ix[k] = 0;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            if (lane + 32u * k + 128u < L && v[k + 4] < v[k]) { v[k] = v[k + 4]; ix[k] = ix[k + 4]; }
-#pragma unroll
-        for (int k = 0; k < 2; k++)
-            if (lane + 32u * k + 64u < L && v[k + 2] < v[k]) { v[k] = v[k + 2]; ix[k] = ix[k + 2]; }
-        if (lane + 32u < L && v[1] < v[0]) { v[0] = v[1]; ix[0] = ix[1]; }
-#pragma unroll
-        for (int s = 16; s > 0; s >>= 1) {
-            const K ov = shfl_down_any(v[0], s);
-            const unsigned long long oi = __shfl_down_sync(0xffffffffu, ix[0], s);
-            if (lane < (uint32_t)s && lane + s < L && ov < v[0]) { v[0] = ov; ix[0] = oi; }
-        }
-        if (lane == 0) { out_v[b] = v[0]; out_i[b] = ix[0]; }
+        K rv;
+        unsigned long long ri;
+        min_tree_warp256<K>(
+            [&](uint32_t t, K& v, unsigned long long& i) {
+                if constexpr (FIRST) { v = RadixKey<K>::value(keys[base + t]); i = base + t; }
+                else { v = in_v[base + t]; i = in_i[base + t]; }
+            },
+            L, rv, ri);
+        if (lane == 0) { out_v[b] = rv; out_i[b] = ri; }
     }
 }
 

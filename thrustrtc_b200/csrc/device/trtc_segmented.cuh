@@ -468,6 +468,160 @@ __global__ void __launch_bounds__(256, MINB) seg_sort_scan_kernel(typename Radix
     }
 }
 
+// ------------------------------------------------------------------ NaN rotation (float keys)
+// The reference sorts a float vector by (code(x) - code(m)) mod 2^w, m the element that its
+// Min_Element tree selects (extrema.cpp:5-13 over internal/general_reduce.cpp:55-95).  With a
+// NaN in a left slot the tree can select a non-minimum, and the sorted order is the code order
+// rotated so that the keys ordered at or above m come first.  A segment sorted on its own gets
+// the same rotation here: seg_rot_kernel (before the sort) replays the tree on every segment
+// that holds a NaN and counts its keys ordered strictly below the selected one;
+// seg_rotate_kernel (after the sort) rotates those segments by that count and redoes their
+// exclusive scans.  Segments without a NaN are only read once, for the NaN test.
+template <class K> struct SegMinSlot {
+    K v;
+    unsigned long long i;
+};
+
+// tree slots of a segment starting at element `base` (index `sid`): the rounds need at most
+// ceil(L/256) + ceil(L/2^16) + ceil(L/2^24) + 1 slots, which fit between base/128 + 4*sid and
+// the next segment's start; the whole area holds n/128 + 4*nseg + 4 slots
+TRTC_FORCEINLINE unsigned long long seg_tree_base(unsigned long long base, unsigned long long sid) {
+    return base / 128ull + 4ull * sid;
+}
+inline unsigned long long seg_tree_slots(unsigned long long n, unsigned long long nseg) {
+    return n / 128ull + 4ull * nseg + 4ull;
+}
+
+template <class K, class OFF>
+__global__ void __launch_bounds__(256) seg_rot_kernel(const typename RadixKey<K>::B* __restrict__ keys,
+                                                      const OFF* __restrict__ off,
+                                                      const SegItem* __restrict__ items, unsigned long long nseg,
+                                                      SegMinSlot<K>* tree, uint32_t* __restrict__ rot) {
+    typedef RadixKey<K> RK;
+    typedef typename RK::B KB;
+    __shared__ unsigned long long s_c[8];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (unsigned long long sid = blockIdx.x; sid < nseg; sid += gridDim.x) {
+        const KB* gk;
+        uint32_t len;
+        unsigned long long base;
+        if (items) {
+            const SegItem it = items[sid];
+            gk = reinterpret_cast<const KB*>(it.k);
+            len = (uint32_t)it.n;
+            base = it.toff;
+        } else {
+            base = (unsigned long long)off[sid];
+            len = (uint32_t)((unsigned long long)off[sid + 1] - base);
+            gk = keys + base;
+        }
+        bool nan = false;
+        for (uint32_t e = threadIdx.x; e < len; e += 256) nan |= RK::is_nan(gk[e]);
+        if (!__syncthreads_or(nan)) {
+            if (threadIdx.x == 0) rot[sid] = 0;
+            continue;
+        }
+        // round 1 over 256-blocks of the keys, then rounds over the block results (slots in
+        // global memory, written and read by this CTA only, ordered by its barriers)
+        SegMinSlot<K>* src = tree + seg_tree_base(base, sid);
+        uint32_t m = (len + 255u) / 256u;
+        for (uint32_t b = warp; b < m; b += 8) {
+            const uint32_t L = min(256u, len - b * 256u);
+            K rv;
+            unsigned long long ri;
+            min_tree_warp256<K>(
+                [&](uint32_t t, K& v, unsigned long long& i) { v = RK::value(gk[b * 256u + t]); i = b * 256u + t; },
+                L, rv, ri);
+            if (lane == 0) { src[b].v = rv; src[b].i = ri; }
+        }
+        __syncthreads();
+        while (m > 1) {
+            SegMinSlot<K>* dst = src + m;
+            const uint32_t nb = (m + 255u) / 256u;
+            for (uint32_t b = warp; b < nb; b += 8) {
+                const uint32_t L = min(256u, m - b * 256u);
+                K rv;
+                unsigned long long ri;
+                min_tree_warp256<K>(
+                    [&](uint32_t t, K& v, unsigned long long& i) { v = src[b * 256u + t].v; i = src[b * 256u + t].i; },
+                    L, rv, ri);
+                if (lane == 0) { dst[b].v = rv; dst[b].i = ri; }
+            }
+            __syncthreads();
+            src = dst;
+            m = nb;
+        }
+        const typename RK::U tm = RK::ordered(gk[src[0].i]);
+        unsigned long long c = 0;
+        for (uint32_t e = threadIdx.x; e < len; e += 256) c += RK::ordered(gk[e]) < tm ? 1ull : 0ull;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(0xffffffffu, c, d);
+        if (lane == 0) s_c[warp] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long t = 0;
+            for (int w = 0; w < 8; w++) t += s_c[w];
+            rot[sid] = (uint32_t)t;
+        }
+        __syncthreads();
+    }
+}
+
+template <class K, class V, class OFF, bool DESC>
+__global__ void __launch_bounds__(256) seg_rotate_kernel(typename RadixKey<K>::B* __restrict__ keys,
+                                                         V* __restrict__ vals, V* __restrict__ scan,
+                                                         typename RadixKey<K>::B* __restrict__ tk,
+                                                         V* __restrict__ tv, const OFF* __restrict__ off,
+                                                         const SegItem* __restrict__ items, unsigned long long nseg,
+                                                         const uint32_t* __restrict__ rot) {
+    typedef typename RadixKey<K>::B KB;
+    constexpr int CH = 1024;
+    __shared__ V s_v[CH], s_o[CH], s_part[8];
+    for (unsigned long long sid = blockIdx.x; sid < nseg; sid += gridDim.x) {
+        const uint32_t r = rot[sid];
+        if (r == 0) continue;
+        KB* gk;
+        V *gv, *gs;
+        uint32_t len;
+        unsigned long long base;
+        if (items) {
+            const SegItem it = items[sid];
+            gk = reinterpret_cast<KB*>(it.k);
+            gv = reinterpret_cast<V*>(it.v);
+            gs = reinterpret_cast<V*>(it.out);
+            len = (uint32_t)it.n;
+            base = it.toff;
+        } else {
+            base = (unsigned long long)off[sid];
+            len = (uint32_t)((unsigned long long)off[sid + 1] - base);
+            gk = keys + base;
+            gv = vals + base;
+            gs = scan + base;
+        }
+        for (uint32_t e = threadIdx.x; e < len; e += 256) { tk[base + e] = gk[e]; tv[base + e] = gv[e]; }
+        __syncthreads();
+        // ascending: sorted position p moves to p - r (mod len); descending: to p + r
+        for (uint32_t e = threadIdx.x; e < len; e += 256) {
+            uint32_t d = DESC ? e + r : e + (len - r);
+            if (d >= len) d -= len;
+            gk[d] = tk[base + e];
+            gv[d] = tv[base + e];
+        }
+        __syncthreads();
+        if (gs) {
+            V carry = V();
+            for (uint32_t cb = 0; cb < len; cb += CH) {
+                const uint32_t cn = min((uint32_t)CH, len - cb);
+                for (uint32_t e = threadIdx.x; e < cn; e += 256) s_v[e] = gv[cb + e];
+                __syncthreads();
+                carry = seg_block_excl_scan<V, CH / 256>(s_v, s_o, cn, carry, s_part);
+                for (uint32_t e = threadIdx.x; e < cn; e += 256) gs[cb + e] = s_o[e];
+                __syncthreads();
+            }
+        }
+    }
+}
+
 // Exclusive Plus scans of many segments (list mode): a persistent CTA takes one segment at
 // a time and scans it in chunks of 256 * ITEMS with a running carry.
 template <class T, int ITEMS>

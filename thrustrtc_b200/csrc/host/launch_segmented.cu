@@ -21,10 +21,16 @@ std::map<int, int> g_seg_items;  // key type -> tuned items per thread
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+template <class K> constexpr bool is_float_key() { return is_same<K, float>::value || is_same<K, double>::value; }
+
+// control block, queue, temp keys, temp values; float keys add the NaN-rotation counts and
+// the Min_Element tree slots (seg_rot_kernel)
 template <class K>
 size_t ws_bytes(size_t n, size_t nseg) {
-    return align256(sizeof(SegCtrl)) + align256(nseg * 4) + align256(n * sizeof(typename RadixKey<K>::B)) +
-           align256(n * 4);
+    size_t b = align256(sizeof(SegCtrl)) + align256(nseg * 4) + align256(n * sizeof(typename RadixKey<K>::B)) +
+               align256(n * 4);
+    if (is_float_key<K>()) b += align256(nseg * 4) + align256(seg_tree_slots(n, nseg) * sizeof(SegMinSlot<K>));
+    return b;
 }
 
 template <class K, bool DESC, int ITEMS>
@@ -40,8 +46,20 @@ bool seg_run_cfg(void* keys, void* vals, void* scan, const unsigned long long* o
     KB* tk = (KB*)p;
     p += align256(n * sizeof(KB));
     V* tv = (V*)p;
+    p += align256(n * 4);
+    uint32_t* rot = (uint32_t*)p;  // float keys only
+    p += align256(nseg * 4);
+    SegMinSlot<K>* tree = (SegMinSlot<K>*)p;
     if (!TRTC_CUDA(cudaMemsetAsync(ctrl, 0, sizeof(SegCtrl), s))) return false;
     const int sms = sm_count();
+    const unsigned rgrid = (unsigned)(nseg < (size_t)sms * 8 ? nseg : (size_t)sms * 8);
+    if constexpr (is_float_key<K>()) {
+        // the reference's per-segment NaN rotation, counted on the unsorted keys
+        ktimer_mark("", s);
+        seg_rot_kernel<K, unsigned long long><<<rgrid, 256, 0, s>>>((const KB*)keys, off, nullptr, nseg, tree, rot);
+        count_launch();
+        ktimer_mark("seg_rot_kernel", s);
+    }
     size_t qg = (nseg + 255) / 256;
     if (qg > (size_t)sms * 4) qg = (size_t)sms * 4;
     if (qg < 1) qg = 1;
@@ -62,6 +80,12 @@ bool seg_run_cfg(void* keys, void* vals, void* scan, const unsigned long long* o
     kernel<<<(unsigned)grid, 256, smem, s>>>((KB*)keys, (V*)vals, (V*)scan, tk, tv, off, queue, nseg, ctrl, nullptr);
     ktimer_mark("seg_sort_scan_kernel", s);
     count_launch(2);
+    if constexpr (is_float_key<K>()) {
+        seg_rotate_kernel<K, V, unsigned long long, DESC><<<rgrid, 256, 0, s>>>((KB*)keys, (V*)vals, (V*)scan, tk, tv,
+                                                                             off, nullptr, nseg, rot);
+        count_launch();
+        ktimer_mark("seg_rotate_kernel", s);
+    }
     return TRTC_CUDA(cudaGetLastError());
 }
 
@@ -105,6 +129,7 @@ __global__ void seg_fill_kernel(uint32_t* k, uint32_t* v, size_t words, unsigned
 }  // namespace
 
 size_t segmented_workspace_bytes(int tc, size_t n, size_t nseg) {
+    if (tc == TC_F32) return ws_bytes<float>(n, nseg);
     return (tc == TC_U64 || tc == TC_I64) ? ws_bytes<uint64_t>(n, nseg) : ws_bytes<uint32_t>(n, nseg);
 }
 

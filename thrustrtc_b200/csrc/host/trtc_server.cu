@@ -168,8 +168,10 @@ private:
     size_t temp_bytes(const Req& r) const {
         const size_t e = esize(r.type);
         if (r.kind == REQ_SORT_BY_KEY) {
-            // plain radix sort: two temp key and value arrays + status; segmented: one of each
-            return r.n > coalesce_max_ ? 2 * r.n * (e + 4) + (r.n / 1024 + 1) * 4096 : a256(r.n * (e + 4));
+            // plain radix sort: two temp key and value arrays + status; segmented: one of each,
+            // plus (float keys) the NaN-rotation tree slots (16 bytes per 128 keys + 4 per request)
+            if (r.n > coalesce_max_) return 2 * r.n * (e + 4) + (r.n / 1024 + 1) * 4096;
+            return a256(r.n * (e + 4)) + (r.type == TC_F32 ? r.n / 8 + 96 : 0);
         }
         return 4096;
     }
@@ -283,7 +285,11 @@ private:
         const size_t ctrl_bytes = a256(sizeof(SegCtrl));
         const size_t res_bytes = a256(g * 8);
         const size_t tk_bytes = a256(tn * e), tv_bytes = a256(tn * 4);
-        const size_t bytes = items_bytes + ctrl_bytes + res_bytes + tk_bytes + tv_bytes;
+        // float sorts: per-request NaN-rotation counts and Min_Element tree slots
+        const bool fsort = h.kind == REQ_SORT_BY_KEY && h.type == TC_F32;
+        const size_t rot_bytes = fsort ? a256(g * 4) : 0;
+        const size_t tree_bytes = fsort ? a256(seg_tree_slots(tn, g) * sizeof(SegMinSlot<float>)) : 0;
+        const size_t bytes = items_bytes + ctrl_bytes + res_bytes + tk_bytes + tv_bytes + rot_bytes + tree_bytes;
         if (!TRTC_CUDA(cudaMallocAsync(&sl.dev, bytes, sl.s))) { sl.dev = nullptr; return false; }
         unsigned char* p = (unsigned char*)sl.dev;
         SegItem* d_items = (SegItem*)p;
@@ -291,6 +297,8 @@ private:
         unsigned long long* d_res = (unsigned long long*)(p + items_bytes + ctrl_bytes);
         void* tk = p + items_bytes + ctrl_bytes + res_bytes;
         void* tv = (unsigned char*)tk + tk_bytes;
+        uint32_t* rot = (uint32_t*)((unsigned char*)tv + tv_bytes);
+        void* tree = (unsigned char*)rot + rot_bytes;
         if (h.kind == REQ_REDUCE)
             for (size_t i = 0; i < g; i++) sl.h_items[i].out = d_res + i;
         if (!TRTC_CUDA(cudaMemcpyAsync(d_items, sl.h_items, g * sizeof(SegItem), cudaMemcpyHostToDevice, sl.s)) ||
@@ -301,7 +309,7 @@ private:
         const unsigned grid = (unsigned)std::min<size_t>(g, (size_t)sms * 2);
         switch (h.kind) {
             case REQ_SORT_BY_KEY: {
-                if (!group_sort(h.type, d_items, g, ctrl, tk, tv, grid, sl.s)) return false;
+                if (!group_sort(h.type, d_items, g, ctrl, tk, tv, rot, tree, grid, sl.s)) return false;
                 break;
             }
             case REQ_EXCL_SCAN: {
@@ -332,8 +340,8 @@ private:
     }
 
     template <class K>
-    static bool group_sort_k(SegItem* items, size_t g, SegCtrl* ctrl, void* tk, void* tv, unsigned grid,
-                             cudaStream_t s) {
+    static bool group_sort_k(SegItem* items, size_t g, SegCtrl* ctrl, void* tk, void* tv, uint32_t* rot, void* tree,
+                             unsigned grid, cudaStream_t s) {
         constexpr int ITEMS = 8;
         typedef typename RadixKey<K>::B KB;
         constexpr size_t smem = seg_sort_scan_smem<K, uint32_t, ITEMS>();
@@ -347,20 +355,32 @@ private:
                 return false;
             attr = true;
         }
+        constexpr bool FK = is_same<K, float>::value;
+        if constexpr (FK) {
+            // the reference's NaN rotation per request (as its own Sort_By_Key call applies it)
+            seg_rot_kernel<K, unsigned long long><<<grid, 256, 0, s>>>(nullptr, nullptr, items, g,
+                                                                       (SegMinSlot<K>*)tree, rot);
+            count_launch();
+        }
         kernel<<<grid, 256, smem, s>>>(nullptr, nullptr, nullptr, (KB*)tk, (uint32_t*)tv, nullptr, nullptr, g, ctrl,
                                        items);
         count_launch();
+        if constexpr (FK) {
+            seg_rotate_kernel<K, uint32_t, unsigned long long, false><<<grid, 256, 0, s>>>(
+                nullptr, nullptr, nullptr, (KB*)tk, (uint32_t*)tv, nullptr, items, g, rot);
+            count_launch();
+        }
         return true;
     }
 
-    static bool group_sort(int type, SegItem* items, size_t g, SegCtrl* ctrl, void* tk, void* tv, unsigned grid,
-                           cudaStream_t s) {
+    static bool group_sort(int type, SegItem* items, size_t g, SegCtrl* ctrl, void* tk, void* tv, uint32_t* rot,
+                           void* tree, unsigned grid, cudaStream_t s) {
         switch (type) {
-            case TC_U32: return group_sort_k<uint32_t>(items, g, ctrl, tk, tv, grid, s);
-            case TC_I32: return group_sort_k<int32_t>(items, g, ctrl, tk, tv, grid, s);
-            case TC_F32: return group_sort_k<float>(items, g, ctrl, tk, tv, grid, s);
-            case TC_I64: return group_sort_k<int64_t>(items, g, ctrl, tk, tv, grid, s);
-            default: return group_sort_k<uint64_t>(items, g, ctrl, tk, tv, grid, s);
+            case TC_U32: return group_sort_k<uint32_t>(items, g, ctrl, tk, tv, rot, tree, grid, s);
+            case TC_I32: return group_sort_k<int32_t>(items, g, ctrl, tk, tv, rot, tree, grid, s);
+            case TC_F32: return group_sort_k<float>(items, g, ctrl, tk, tv, rot, tree, grid, s);
+            case TC_I64: return group_sort_k<int64_t>(items, g, ctrl, tk, tv, rot, tree, grid, s);
+            default: return group_sort_k<uint64_t>(items, g, ctrl, tk, tv, rot, tree, grid, s);
         }
     }
 
