@@ -27,6 +27,11 @@ unsigned long long trtc_launch_count(void);
 void trtc_timing_enable(int on);
 int trtc_timing_count(void);
 int trtc_timing_get(int i, char* name, unsigned long long name_cap, float* ms);
+/* caps the size of any one device allocation the library makes for a call (temporaries and
+ * DVVector storage; 0 removes the cap).  An allocation above the cap fails the way an
+ * out-of-memory one does (the call returns its failure value, before any kernel runs, and
+ * leaves its inputs untouched); for capacity planning and for tests of those failure paths. */
+void trtc_set_alloc_limit(unsigned long long bytes);
 /* synchronises `stream`; 0, or -1 when a kernel reported an error */
 int trtc_raw_sync(void* stream);
 
@@ -89,6 +94,13 @@ int trtc_raw_segmented_sort_scan(int key_type, void* keys, void* values, void* s
  * chosen items per thread, or -1.  Allocates its own scratch; synchronous. */
 int trtc_raw_segmented_autotune(int key_type, const unsigned long long* offsets, unsigned long long nseg,
                                 unsigned long long n, void* stream);
+
+/* Test hook for the bounded device waits: one inclusive Plus scan of int32 (n >= 4 * 8192)
+ * with a kernel built so that tile 2 never publishes its look-back word and every wait gives
+ * up after 4096 polls.  The waits behind tile 2 run out, the kernel records the error and
+ * finishes; the call returns -1 with "look-back wait exceeded its bound" in
+ * trtc_last_error(), and the library stays usable (out holds garbage).  Synchronous. */
+int trtc_test_scan_lookback_timeout(const int* in, int* out, unsigned long long n, void* stream);
 
 /* diagnostics: copies the sort control block of the last sort on `stream` */
 unsigned long long trtc_debug_sort_ctrl(void* host, unsigned long long bytes, void* stream);

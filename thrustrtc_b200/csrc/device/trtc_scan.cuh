@@ -11,6 +11,13 @@
 // array never needs clearing between calls.  Operators need only be associative: all
 // combinations keep index order (older operand on the left), no identity element is used.
 #pragma once
+
+// Test hook of the two-phase scan: a build that defines TRTC_FAULT_SKIP_PUBLISH(tile) true for
+// some tile leaves that tile's look-back word unpublished, so the bounded waits of the tiles
+// after it run out (launch_faultinject.cu).  Every other build leaves it false.
+#ifndef TRTC_FAULT_SKIP_PUBLISH
+#define TRTC_FAULT_SKIP_PUBLISH(tile) false
+#endif
 #include "trtc_prelude.cuh"
 #include "trtc_builtins.cuh"
 #include "trtc_abi.h"
@@ -533,7 +540,7 @@ __global__ void __launch_bounds__(BLOCK) scan2_kernel(const T* __restrict__ in, 
                 opt_combine(incl, incl_h, agg, agg_h, op);
                 publish<T>(st, 0, incl, true, false);
             } else {
-                publish<T>(st, tile, agg, false, false);
+                if (!TRTC_FAULT_SKIP_PUBLISH(tile)) publish<T>(st, tile, agg, false, false);
             }
         }
     };
@@ -560,7 +567,7 @@ __global__ void __launch_bounds__(BLOCK) scan2_kernel(const T* __restrict__ in, 
                 T incl = tp;
                 bool incl_h = tp_h;
                 opt_combine(incl, incl_h, s_agg[buf], s_agg_h[buf] != 0, op);
-                if (lane == 0) publish<T>(st, cur, incl, true, false);
+                if (lane == 0 && !TRTC_FAULT_SKIP_PUBLISH(cur)) publish<T>(st, cur, incl, true, false);
             }
             if (lane == 0) { s_pre = tp; s_pre_h = tp_h ? 1 : 0; }
         }

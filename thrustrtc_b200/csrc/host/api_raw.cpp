@@ -40,6 +40,8 @@ unsigned long long trtc_debug_sort_ctrl(void* host, unsigned long long bytes, vo
     return bytes;
 }
 
+void trtc_set_alloc_limit(unsigned long long bytes) { set_alloc_limit(bytes); }
+
 int trtc_raw_sync(void* stream) {
     if (!ensure_device()) return -1;
     return check_device_errors(S(stream), "stream") ? 0 : -1;

@@ -253,9 +253,22 @@ void* sort_ctrl_ws(cudaStream_t s, size_t bytes) {
     return w->sort_ctrl;
 }
 
+// ---------------------------------------------------------------- allocation cap
+static std::atomic<unsigned long long> g_alloc_limit{0};
+void set_alloc_limit(unsigned long long bytes) { g_alloc_limit.store(bytes, std::memory_order_relaxed); }
+
+static bool within_alloc_limit(size_t bytes, const char* what) {
+    const unsigned long long lim = g_alloc_limit.load(std::memory_order_relaxed);
+    if (lim == 0 || bytes <= lim) return true;
+    set_error(std::string(what) + ": allocation of " + std::to_string(bytes) + " bytes exceeds the limit of " +
+              std::to_string(lim) + " bytes (trtc_set_alloc_limit)");
+    return false;
+}
+
 void* tmp_alloc(size_t bytes, cudaStream_t s) {
     void* p = nullptr;
     if (bytes == 0) bytes = 16;
+    if (!within_alloc_limit(bytes, "temporary")) return nullptr;
     if (!TRTC_CUDA(cudaMallocAsync(&p, bytes, s))) return nullptr;
     return p;
 }
@@ -265,6 +278,7 @@ void tmp_free(void* p, cudaStream_t s) {
 
 void* vector_alloc(size_t bytes) {
     void* p = nullptr;
+    if (!within_alloc_limit(bytes, "vector")) return nullptr;
     if (!g_vec_pool) return TRTC_CUDA(cudaMalloc(&p, bytes)) ? p : nullptr;
     // ordered on the legacy default stream, like the copy or memset that fills the vector
     if (cudaMallocFromPoolAsync(&p, bytes, g_vec_pool, 0) == cudaSuccess) return p;

@@ -65,6 +65,9 @@ LookbackWs* lookback_ws(cudaStream_t s, size_t tiles, size_t value_size, uint32_
 LookbackWs* reduce_ws(cudaStream_t s, size_t partials, size_t value_size);
 void* sort_ctrl_ws(cudaStream_t s, size_t bytes);
 
+// cap on the size of any one temporary or vector allocation (0: none); an allocation above it
+// fails like an out-of-memory one, before anything is launched
+void set_alloc_limit(unsigned long long bytes);
 // stream-ordered temporaries (cached by the CUDA memory pool)
 void* tmp_alloc(size_t bytes, cudaStream_t s);
 void tmp_free(void* p, cudaStream_t s);
