@@ -46,18 +46,26 @@ unsigned long long trtc_raw_min_element(int type, const void* in, unsigned long 
 /* inclusive (exclusive=0) or exclusive scan with host-side init (NULL: zero) */
 int trtc_raw_scan(int type, int op, int exclusive, const void* in, void* out, unsigned long long n,
                   const void* init, void* stream);
-/* trtc_raw_scan without allocation.  No counterpart in the reference: ThrustRTC allocates
- * its scan workspace on every call.  Same kernel and results as trtc_raw_scan for int32 (4),
+/* trtc_raw_scan without any allocation.  No counterpart in the reference, which allocates
+ * scan workspace on every call.  For callers that cannot allocate device memory while they
+ * run: code inside a memory-pool or allocator callback (an allocation would re-enter the
+ * allocator), a framework that has reserved the device's memory for its own allocator (a
+ * cudaMalloc would fail), or a real-time loop that cannot take cudaMalloc's device-wide
+ * synchronisation.  It runs the two-phase kernel trtc_raw_scan runs for these types; integer
+ * results are identical to trtc_raw_scan's, float results agree within rounding (a float
+ * look-back may group tile totals differently from one run to the next).  Accepts int32 (4),
  * uint32 (5) and float (8), op 0 Plus / 1 Maximum / 2 Minimum, 1 <= n <= 2^28 elements; other
- * sizes or types return -1 with a message in trtc_last_error() and launch nothing.  The
- * look-back scratch is a 512 KiB array in the library's static device memory: the call
- * allocates nothing (no cudaMalloc, cudaFree, pinned host memory or memory pool).  The first
- * call on a device does a one-time set-up (the scratch array's address) and should precede
- * stream capture.  status_dev: NULL, or a caller-owned device word that must be zero before
- * the call; a device-side failure (an expired bounded wait) ORs a nonzero code into it.
- * Calls share one scratch array per device, so calls that overlap on the device (other
- * streams, other host threads) race: issue them in one stream or synchronise in between.
- * Asynchronous with respect to the host. */
+ * sizes, types or operators return -1 with a message in trtc_last_error() and launch
+ * nothing.  The look-back scratch is a 256 KiB array in the library's static device memory,
+ * held by every GPU context that loads the library until the process exits; the call makes
+ * no cudaMalloc, cudaFree, pinned host allocation or memory-pool allocation.  The first call
+ * in a CUDA context does a one-time set-up (it looks up the scratch array's device address
+ * with that context current); make that first call before any stream capture.  Every call
+ * shares the one scratch array of its context, which keeps the last call's contents, so
+ * calls that overlap on the device (other streams, other host threads) race: issue them in
+ * one stream or synchronise in between.  status_dev: NULL, or a caller-owned device word that
+ * must be zero before the call; a device-side failure (an expired bounded wait) ORs a
+ * nonzero code into it.  Asynchronous with respect to the host. */
 int trtc_raw_scan_noalloc(int type, int op, int exclusive, const void* in, void* out, unsigned long long n,
                           const void* init, unsigned int* status_dev, void* stream);
 /* reduction to host memory (init may be NULL); synchronous */
