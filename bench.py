@@ -18,6 +18,9 @@ One JSON line on rank 0:
   roofline     the dominant kernel's algorithmic bytes per launch / its average device time
                (per-launch CUDA events recorded by the library over the timed region)
   cpu_baseline the oracle's host sort / scan / reduce on a bounded sample, all host threads
+  configs      (default run) the same record for the inclusive scan of 2^28 int32 and the
+               reduce of 2^28 float32, and the serving form: both paths' capacity and their
+               p50 / p99 latency on one grid of offered request rates
 
 `--impl reference` times the reference algorithm's CPU restatement (the reference itself has
 no CPU path and does not build here) on the same workload definition.
@@ -355,13 +358,43 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     import thrustrtc_b200 as trtc
-    from thrustrtc_b200 import _native as N
     trtc.init()
-    L = N.lib
-    wl = args.workload
-    n, kname, b_launch, b_unit, metric, unit = WORKLOADS[wl]
-    n = args.n or n
     assert args.warmup >= 3 or args.allow_short_warmup, "at least 3 warm-up steps"
+
+    line = _measure_plain(args.workload, args, dev, rank, world, with_e2e=not args.no_e2e,
+                          with_cpu=not args.no_cpu)
+    if args.workload == "sort_by_key_u32" and not args.no_sub:
+        # the other configurations of the headline metric, measured in the same run:
+        # C2b scan and C2c reduce (replicas on every rank, max over ranks), and the serving
+        # form (rank 0 of a one-GPU run only: the serving loop is a one-GPU measurement)
+        sub = {}
+        for wl in ("inclusive_scan_i32", "reduce_f32"):
+            sub[wl] = _measure_plain(wl, args, dev, rank, world, with_e2e=not args.no_e2e,
+                                     with_cpu=not args.no_cpu)
+        if world == 1:
+            sub["serving_c5"] = _serving_measure(args.sub_requests, dev, shared_grid=True)
+        else:
+            sub["serving_c5"] = {"skipped": "one-GPU measurement; run with --gpus 1"}
+        if line is not None:
+            line["configs"] = sub
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def _measure_plain(wl, args, dev, rank, world, with_e2e=True, with_cpu=True):
+    """One plain workload (sort_by_key_u32 / inclusive_scan_i32 / reduce_f32): warm-up, K
+    timed steps on the legacy default stream, correctness check, roofline of the dominant
+    kernel, end-to-end line and CPU baseline.  Returns the JSON record on rank 0 (else None)."""
+    import torch
+    from thrustrtc_b200 import _native as N
+    L = N.lib
+    n, kname, b_launch, b_unit, metric, unit = WORKLOADS[wl]
+    n = (args.n or n) if wl == args.workload else n
 
     keys_h, vals_h = gen_inputs(wl, n)
     stream = None  # the legacy default stream: torch's current stream and the library's
@@ -459,35 +492,30 @@ def run_ours(args):
 
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
-    if not args.no_e2e:
+    if with_e2e:
         e2e = _e2e(args, wl, n, keys_h, vals_h, world, max_over_ranks, barrier)
 
     cpu = None
-    if world == 1 and rank == 0 and not args.no_cpu:
+    if world == 1 and rank == 0 and with_cpu:
         threads = cpu_threads()
         sample = args.cpu_sample or (1 << 25 if wl == "sort_by_key_u32" else 1 << 27)
         sample = min(sample, n)
         secs, threads, _ = cpu_run(wl, sample, threads)
         cpu = {"value": units_per_s_to_metric(wl, sample, secs), "unit": unit, "cores": threads, "kind": "port",
                "sample": "first %d units of the same workload, oracle host restatement, %d threads" % (sample, threads)}
-
-    if world > 1:
-        torch.distributed.barrier()
-    if rank == 0:
-        line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": _dtype(wl),
-                "data": "synthetic (SplitMix64 seed 0, generated on the host)", "config": _config(wl, n, world),
-                "roofline": roofline,
-                "roofline_whole_op": {"algorithmic_bytes_per_unit": b_unit, "achieved": whole,
-                                      "frac": whole / peak, "unit": "GB/s"},
-                "kernel_ms_timed_region": {k2: round(v2, 4) for k2, v2 in sorted(kernel_share.items())},
-                "cpu_baseline": cpu, "e2e": e2e, "clocks": sampler.summary(), "gpu_launches": launches,
-                "step_ms": [round(s, 4) for s in step_ms]}
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.destroy_process_group()
-    return 0
+    del keys_h, vals_h
+    if rank != 0:
+        return None
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": _dtype(wl),
+            "data": "synthetic (SplitMix64 seed 0, generated on the host)", "config": _config(wl, n, world),
+            "roofline": roofline,
+            "roofline_whole_op": {"algorithmic_bytes_per_unit": b_unit, "achieved": whole,
+                                  "frac": whole / peak, "unit": "GB/s"},
+            "kernel_ms_timed_region": {k2: round(v2, 4) for k2, v2 in sorted(kernel_share.items())},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": sampler.summary(), "gpu_launches": launches,
+            "step_ms": [round(s, 4) for s in step_ms]}
 
 
 def _check(wl, n, env):
@@ -1035,11 +1063,11 @@ def _srv_sigs(L):
     L.trtc_server_destroy.argtypes = [ctypes.c_void_p]
 
 
+SERVING_GRID = (0.25, 0.50, 0.75, 0.90, 1.00, 1.25, 1.50, 2.00, 2.50)
+
+
 def run_serving(args):
-    """Poisson arrivals of mixed requests into the request server (continuous batching: 8
-    streams, coalescing of requests up to 2^16 elements, 32 GB admission budget) beside the
-    plain path (the same requests one call at a time, no coalescing, one stream).  Offered
-    load is swept over fractions of each path's closed-loop capacity."""
+    """The serving form as its own JSON line (see _serving_measure)."""
     import torch
     rank, world, local = dist_env()
     if not torch.cuda.is_available():
@@ -1048,58 +1076,96 @@ def run_serving(args):
         return 0  # one GPU: the serving form is measured on rank 0 only
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    count = args.n or WORKLOADS["serving_c5"][0]
+    levels = tuple(float(f) for f in args.levels.split(",")) if args.levels else SERVING_GRID
+    rec = _serving_measure(count, dev, shared_grid=True, grid=levels)
+    line = {"metric": WORKLOADS["serving_c5"][4], "value": rec["capacity_rps"]["served"], "unit": "requests/s",
+            "n_gpus": 1, "steps": len(rec["levels"]), "warmup": 1,
+            "ms_per_step": 1e3 * 1000 / rec["capacity_rps"]["served"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32/i64/f32",
+            "data": "synthetic (SplitMix64 seed 0 request mix; torch generator seed 0 contents)",
+            "config": rec["config"], "capacity_rps": rec["capacity_rps"], "levels": rec["levels"],
+            "clocks": rec["clocks"], "gpu_launches": rec["gpu_launches"],
+            "e2e": None, "cpu_baseline": None, "roofline": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _serving_measure(count, dev, shared_grid=True, grid=SERVING_GRID, block=1000):
+    """Poisson arrivals of `count` mixed requests into the request server (continuous
+    batching: 8 streams, coalescing of requests up to 2^16 elements, 32 GB admission budget)
+    beside the plain path (the same requests one call at a time on one stream, no coalescing).
+
+    Capacity: each path's closed-loop throughput on the first block of requests (all
+    submitted at once).  Latency: offered rates on one grid for both paths (fractions of the
+    plain path's capacity, shared_grid=True) or each path at fractions of its own capacity;
+    p50 / p99 of submit-to-done latency over all requests.  Streams longer than `block`
+    requests run block after block (inputs restored between blocks, queues drained), so the
+    device buffers stay the size of one block."""
+    import torch
     import thrustrtc_b200 as trtc
     from thrustrtc_b200 import _native as N
     trtc.init()
     L = N.lib
     _srv_sigs(L)
-    count = args.n or WORKLOADS["serving_c5"][0]
     reqs = serving_requests(count)
-    # device inputs: one pristine and one working slice per request, per element type
-    tot = {5: 0, 6: 0, 8: 0}
-    offs = []
-    for kind, t, n in reqs:
-        offs.append(tot[t])
-        tot[t] += n
+    block = min(block, count)
+    blocks = [reqs[i:i + block] for i in range(0, count, block)]
+    esz = {5: 4, 6: 8, 8: 4}
+    # capacity per element type (and of the value array) for the largest block
+    cap_t = {5: 1, 6: 1, 8: 1}
+    cap_v = 1
+    for b in blocks:
+        tot = {5: 0, 6: 0, 8: 0}
+        for kind, t, n in b:
+            tot[t] += n
+        for t in tot:
+            cap_t[t] = max(cap_t[t], tot[t])
+        cap_v = max(cap_v, sum(n for k, t, n in b if k == 0))
     g = torch.Generator(device=dev)
     g.manual_seed(0)
-    pristine = {5: torch.randint(-2**31, 2**31 - 1, (max(tot[5], 1),), dtype=torch.int32, device=dev, generator=g),
-                6: torch.randint(-2**62, 2**62, (max(tot[6], 1),), dtype=torch.int64, device=dev, generator=g),
-                8: torch.randn(max(tot[8], 1), device=dev, generator=g)}
+    pristine = {5: torch.randint(-2**31, 2**31 - 1, (cap_t[5],), dtype=torch.int32, device=dev, generator=g),
+                6: torch.randint(-2**62, 2**62, (cap_t[6],), dtype=torch.int64, device=dev, generator=g),
+                8: torch.randn(cap_t[8], device=dev, generator=g)}
     work = {t: torch.empty_like(x) for t, x in pristine.items()}
-    vals = torch.empty(sum(n for k, t, n in reqs if k == 0) + 1, dtype=torch.int32, device=dev)
     outs = {t: torch.empty_like(x) for t, x in pristine.items()}
-    voff, acc = [], 0
-    for kind, t, n in reqs:
-        voff.append(acc)
-        acc += n if kind == 0 else 0
-    esz = {5: 4, 6: 8, 8: 4}
+    vals = torch.empty(cap_v + 1, dtype=torch.int32, device=dev)
+    vals0 = torch.arange(cap_v + 1, dtype=torch.int32, device=dev)
 
-    def ptrs(i):
-        kind, t, n = reqs[i]
-        k = ctypes.c_void_p(work[t].data_ptr() + esz[t] * offs[i])
-        v = ctypes.c_void_p(vals.data_ptr() + 4 * voff[i]) if kind == 0 else None
-        o = ctypes.c_void_p(outs[t].data_ptr() + esz[t] * offs[i]) if kind == 1 else None
-        return k, v, o
+    def layout(b):
+        """Pointers of each request of block b inside the work / value / output buffers."""
+        offs, vof = {5: 0, 6: 0, 8: 0}, 0
+        ptr = []
+        for kind, t, n in b:
+            k = ctypes.c_void_p(work[t].data_ptr() + esz[t] * offs[t])
+            v = ctypes.c_void_p(vals.data_ptr() + 4 * vof) if kind == 0 else None
+            o = ctypes.c_void_p(outs[t].data_ptr() + esz[t] * offs[t]) if kind == 1 else None
+            ptr.append((kind, t, n, k, v, o))
+            offs[t] += n
+            vof += n if kind == 0 else 0
+        return ptr
+
+    layouts = [layout(b) for b in blocks]
 
     def restore():
         for t in work:
             work[t].copy_(pristine[t])
-        vals.copy_(torch.arange(vals.numel(), dtype=torch.int32, device=dev))
+        vals.copy_(vals0)
         torch.cuda.synchronize()
 
-    def run_once(srv, arrivals):
-        """Submits request i at arrivals[i] (seconds from the start; None = all at once) and
-        polls until all are done; returns (latencies in s, makespan in s)."""
+    def run_block(srv, bi, arrivals):
+        """Submits request i of block bi at arrivals[i] (seconds from the block's start;
+        None = all at once) and polls until all are done; returns (latencies, makespan)."""
         restore()
-        ids = [0] * count
+        ptr = layouts[bi]
+        cnt = len(ptr)
+        ids = [0] * cnt
         t0 = L.trtc_server_now(srv)
         nxt = 0
         while True:
             now = L.trtc_server_now(srv) - t0
-            while nxt < count and (arrivals is None or arrivals[nxt] <= now):
-                k, v, o = ptrs(nxt)
-                kind, t, n = reqs[nxt]
+            while nxt < cnt and (arrivals is None or arrivals[nxt] <= now):
+                kind, t, n, k, v, o = ptr[nxt]
                 ids[nxt] = L.trtc_server_submit(srv, kind, t, k, v, o, n)
                 if ids[nxt] <= 0:
                     raise RuntimeError(N.last_error())
@@ -1107,7 +1173,7 @@ def run_serving(args):
             left = L.trtc_server_poll(srv)
             if left < 0:
                 raise RuntimeError(N.last_error())
-            if nxt == count and left == 0:
+            if nxt == cnt and left == 0:
                 break
         lat, first, last = [], None, 0.0
         ts, td = ctypes.c_double(), ctypes.c_double()
@@ -1121,53 +1187,63 @@ def run_serving(args):
         L.trtc_server_forget_done(srv)
         return np.array(lat), last - first
 
-    def sweep(srv):
-        run_once(srv, None)  # warm-up (kernel set-up, memory pool)
-        _, span = run_once(srv, None)
-        cap = count / span
-        levels = []
-        for f in (0.10, 0.25, 0.50, 0.75, 0.90, 1.00, 1.10, 1.20):
-            rate = f * cap
-            h = splitmix64(1, 3, count)
+    def capacity(srv):
+        run_block(srv, 0, None)  # warm-up (kernel set-up, memory pool)
+        _, span = run_block(srv, 0, None)
+        return len(blocks[0]) / span
+
+    def at_rate(srv, rate):
+        lat, span = [], 0.0
+        for bi, b in enumerate(blocks):
+            h = splitmix64(1 + bi, 3, len(b))
             u = ((h >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
             arrivals = np.cumsum(-np.log(u) / rate)
-            lat, span = run_once(srv, arrivals)
-            levels.append({"load": f, "offered_rps": rate, "achieved_rps": count / span,
-                           "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)})
-        return cap, levels
+            lb, sb = run_block(srv, bi, arrivals)
+            lat.append(lb)
+            span += sb
+        lat = np.concatenate(lat)
+        return {"achieved_rps": count / span, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3)}
 
     budget = 32 << 30
-    srv = L.trtc_server_create(budget, 8, 1 << 16)
-    if not srv:
+    served = L.trtc_server_create(budget, 8, 1 << 16)
+    plain = L.trtc_server_create(budget, 1, 0)
+    if not served or not plain:
         raise RuntimeError(N.last_error())
     lc0 = N.launch_count()
     sampler = ClockSampler(dev)
-    with sampler:
-        cap_b, lv_b = sweep(srv)
+    try:
+        with sampler:
+            cap_b = capacity(served)
+            cap_p = capacity(plain)
+            levels = []
+            for f in grid:
+                if shared_grid:
+                    rate = f * cap_p
+                    levels.append({"offered_rps": rate, "fraction_of_plain_capacity": f,
+                                   "served": at_rate(served, rate), "plain": at_rate(plain, rate)})
+                else:
+                    levels.append({"fraction_of_own_capacity": f, "served": at_rate(served, f * cap_b),
+                                   "plain": at_rate(plain, f * cap_p)})
+    finally:
+        L.trtc_server_destroy(served)
+        L.trtc_server_destroy(plain)
     launches = N.launch_count() - lc0
-    L.trtc_server_destroy(srv)
-    srv = L.trtc_server_create(budget, 1, 0)
-    cap_p, lv_p = sweep(srv)
-    L.trtc_server_destroy(srv)
     elems = sum(n for _, _, n in reqs)
-    line = {"metric": WORKLOADS["serving_c5"][4], "value": cap_b, "unit": "requests/s", "n_gpus": 1,
-            "steps": len(lv_b), "warmup": 1, "ms_per_step": 1e3 * count / cap_b, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32/i64/f32",
-            "data": "synthetic (SplitMix64 seed 0 request mix; torch generator seed 0 contents)",
-            "config": {"workload": "serving_c5", "requests_per_level": count,
-                       "sample": "%d requests per load level (a bounded sample of the 200,000-request stream)" % count,
+    return {"capacity_rps": {"served": cap_b, "plain": cap_p, "ratio": cap_b / cap_p},
+            "levels": levels, "clocks": sampler.summary(), "gpu_launches": launches,
+            "config": {"workload": "serving_c5", "requests": count, "block": block,
+                       "sample": ("the full %d-request stream" % count) if count >= 200000 else
+                                 ("%d requests per load level (a bounded sample of the 200,000-request stream)"
+                                  % count),
                        "mix": "60% Sort_By_Key (+uint32 values), 25% exclusive scan, 15% reduce",
                        "sizes": "log-uniform 2^10..2^24", "types": "uint32 / int64 / float equal shares",
-                       "elements_per_level": elems, "budget_bytes": budget,
+                       "elements": elems, "budget_bytes": budget,
                        "server": "8 streams, coalescing up to 2^16 elements per request, admission by budget",
                        "plain": "same requests, one call at a time on one stream, no coalescing",
-                       "load_levels": "fractions of each path's closed-loop capacity"},
-            "capacity_rps": {"served": cap_b, "plain": cap_p, "ratio": cap_b / cap_p},
-            "levels_served": lv_b, "levels_plain": lv_p,
-            "clocks": sampler.summary(), "gpu_launches": launches,
-            "e2e": None, "cpu_baseline": None, "roofline": None}
-    print(json.dumps(line), flush=True)
-    return 0
+                       "grid": ("the same offered rates for both paths, as fractions of the plain path's "
+                                "capacity") if shared_grid else "fractions of each path's own capacity",
+                       "capacity": "closed loop on the first %d requests, all submitted at once" % len(blocks[0])}}
 
 
 def main():
@@ -1184,6 +1260,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--allow-short-warmup", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="segmented_c4: skip the per-segment plain calls")
+    ap.add_argument("--no-sub", action="store_true", help="default run: skip the scan / reduce / serving records")
+    ap.add_argument("--sub-requests", type=int, default=1000, help="requests of the serving record")
+    ap.add_argument("--levels", default="", help="serving_c5: comma-separated fractions of the plain capacity")
     args = ap.parse_args()
     _, world, _ = dist_env()
     if args.gpus != world and not (args.gpus == 1 and world == 1):
