@@ -97,11 +97,24 @@ unsigned long long trtc_raw_segmented_workspace_bytes(int key_type, unsigned lon
 int trtc_raw_segmented_sort_scan(int key_type, void* keys, void* values, void* scan_out,
                                  const unsigned long long* offsets, unsigned long long nseg, unsigned long long n,
                                  void* workspace, unsigned long long workspace_bytes, int descending, void* stream);
-/* Times the tile configurations (256 x 8 or 256 x 16 keys for the on-chip class) on random
- * keys with these segment offsets and keeps the faster one for this key type; returns the
- * chosen items per thread, or -1.  Allocates its own scratch; synchronous. */
+/* Size classes of the batched kernel: segments of at most `warp_small` (0 or 32) keys are
+ * sorted by one warp with a bitonic network (no digit counters), at most 32 x items keys by
+ * one warp with 8-bit radix passes, at most 256 x items keys by a whole CTA on chip, longer
+ * ones by a whole CTA through global memory; items is 8 or 16.  Per key type, the shape
+ * (items, warp_small) comes from a tuning table: compiled-in defaults (16, 32), a table loaded
+ * from the file named by TRTC_SEG_TUNING_FILE at the first batched call, a table passed to
+ * trtc_raw_segmented_tuning_load, or the autotuner.
+ * The autotuner times the four shapes on random keys with these segment offsets and keeps the
+ * fastest for this key type; returns its items per thread, or -1.  Allocates its own
+ * scratch; synchronous. */
 int trtc_raw_segmented_autotune(int key_type, const unsigned long long* offsets, unsigned long long nseg,
                                 unsigned long long n, void* stream);
+/* the tuning table as versioned JSON (written into out, at most cap bytes with the final NUL);
+ * returns the full length */
+unsigned long long trtc_raw_segmented_tuning_json(char* out, unsigned long long cap);
+/* replaces the entries named in a table of that JSON form; 0, or -1 for another format or
+ * version or an unsupported shape */
+int trtc_raw_segmented_tuning_load(const char* json);
 
 /* Test hook for the bounded device waits: one inclusive Plus scan of int32 (n >= 4 * 8192)
  * with a kernel built so that tile 2 never publishes its look-back word and every wait gives

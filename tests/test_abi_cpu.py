@@ -118,3 +118,28 @@ def test_every_reference_export_is_present():
     lib = ctypes.CDLL(LIB)
     missing = [n for n in names if not hasattr(lib, n)]
     assert missing == []
+
+
+def test_segmented_tuning_table_round_trip():
+    # the batched kernel's size-class table: versioned JSON in, the same entries out; another
+    # format, version or an unsupported shape is refused (host-only, no GPU needed)
+    lib = ctypes.CDLL(LIB)
+    lib.trtc_raw_segmented_tuning_json.restype = ctypes.c_ulonglong
+    lib.trtc_raw_segmented_tuning_json.argtypes = [ctypes.c_char_p, ctypes.c_ulonglong]
+    lib.trtc_raw_segmented_tuning_load.restype = ctypes.c_int
+    lib.trtc_raw_segmented_tuning_load.argtypes = [ctypes.c_char_p]
+    import json
+    t = {"format": "thrustrtc_b200.segmented_tuning", "version": 1,
+         "entries": [{"key_type": 5, "items": 8, "warp_small": 32}, {"key_type": 6, "items": 16, "warp_small": 0}]}
+    assert lib.trtc_raw_segmented_tuning_load(json.dumps(t).encode()) == 0
+    buf = ctypes.create_string_buffer(4096)
+    size = lib.trtc_raw_segmented_tuning_json(buf, 4096)
+    out = json.loads(buf.value.decode())
+    assert size == len(buf.value) and out["version"] == 1 and out["digit_bits"] == 8
+    got = {e["key_type"]: (e["items"], e["warp_small"]) for e in out["entries"]}
+    assert got[5] == (8, 32) and got[6] == (16, 0)
+    bad = dict(t, version=2)
+    assert lib.trtc_raw_segmented_tuning_load(json.dumps(bad).encode()) == -1
+    bad = dict(t, entries=[{"key_type": 5, "items": 12, "warp_small": 32}])
+    assert lib.trtc_raw_segmented_tuning_load(json.dumps(bad).encode()) == -1
+    assert lib.trtc_raw_segmented_tuning_load(b'{"format": "other", "version": 1}') == -1

@@ -23,6 +23,10 @@ def N(cuda):
     L.trtc_raw_segmented_sort_scan.restype = ctypes.c_int
     L.trtc_raw_segmented_sort_scan.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + \
         [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_void_p]
+    L.trtc_raw_segmented_tuning_json.restype = ctypes.c_ulonglong
+    L.trtc_raw_segmented_tuning_json.argtypes = [ctypes.c_char_p, ctypes.c_ulonglong]
+    L.trtc_raw_segmented_tuning_load.restype = ctypes.c_int
+    L.trtc_raw_segmented_tuning_load.argtypes = [ctypes.c_char_p]
     L.trtc_raw_segmented_autotune.restype = ctypes.c_int
     L.trtc_raw_segmented_autotune.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong,
                                               ctypes.c_ulonglong, ctypes.c_void_p]
@@ -187,3 +191,37 @@ def test_segmented_float_nan_rotation(N, desc):
     assert gk.tobytes() == ek.tobytes()
     assert np.array_equal(gv, ev)
     assert np.array_equal(gs, es)
+
+
+SHAPES = [(8, 0), (8, 32), (16, 0), (16, 32)]
+
+
+@pytest.mark.parametrize("items,warp_small", SHAPES)
+@pytest.mark.parametrize("name", ["uint32_t", "float", "int64_t"])
+def test_every_size_class_of_every_shape(N, items, warp_small, name):
+    # a table forcing each shape; lengths on both sides of every class limit of that shape:
+    # the bitonic warp class (<= 32), the radix warp class (<= 32 * items), the on-chip CTA
+    # class (<= 256 * items) and the global-memory CTA class
+    table = ('{"format": "thrustrtc_b200.segmented_tuning", "version": 1, "entries": '
+             '[{"key_type": %d, "items": %d, "warp_small": %d}]}' % (TC[name], items, warp_small))
+    old = ctypes.create_string_buffer(4096)
+    N.lib.trtc_raw_segmented_tuning_json(old, 4096)
+    assert N.lib.trtc_raw_segmented_tuning_load(table.encode()) == 0
+    try:
+        rng = np.random.default_rng(items + warp_small + len(name))
+        lims = [1, 2, 31, 32, 33, 32 * items - 1, 32 * items, 32 * items + 1, 256 * items - 1, 256 * items,
+                256 * items + 1, 3 * 256 * items + 17]
+        lens = np.array(lims + list(make_lengths(rng, 200, 40, 1.5, 6000)), dtype=np.int64)
+        rng.shuffle(lens)
+        off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        n = int(off[-1])
+        keys = keys_for(rng, name, n)
+        vals = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        for desc in (False, True):
+            gk, gv, gs = run(N, name, keys, vals, off, desc)
+            ek, ev, es = expected(keys, vals, off, desc)
+            assert gk.tobytes() == ek.tobytes()
+            assert np.array_equal(gv, ev)
+            assert np.array_equal(gs, es)
+    finally:
+        N.lib.trtc_raw_segmented_tuning_load(old.value)

@@ -4,7 +4,13 @@
 //
 // The reference sorts one vector per call (internal/radix_sort.cpp:165-553) and scans one
 // vector per call (internal/general_scan.cpp:8-88); a batch there is one call pair per
-// segment.  Here a CTA takes a segment id from the queue and sorts the whole segment itself:
+// segment.  Here a CTA takes a segment id from the queue and sorts the whole segment itself,
+// in one of four size classes (the limits are the tuning table's; launch_segmented.cu):
+//   * segments of at most `warp_small` (0 or 32) keys: one warp, a bitonic network over
+//     (code, index) pairs, no digit counters (seg_warp_bitonic);
+//   * segments of at most 32 * ITEMS keys: one warp, four 8-bit LSD passes of ballot
+//     ranking with per-warp counters (seg_warp_sort_scan); a CTA's eight warps take eight
+//     such segments at once;
 //   * small segments (<= 256 * ITEMS keys) are sorted on chip: four 8-bit LSD passes of
 //     warp multisplit ranking + shared-memory scatter, with the tile re-laid out so that
 //     every warp gets keys whatever the segment length; then the values are scanned and
@@ -242,6 +248,55 @@ __device__ inline void seg_warp_sort_scan(typename RadixKey<K>::B* gk, V* gv, V*
     }
 }
 
+// One warp sorts (and scans) a segment of len <= 32 keys without digit counters: a bitonic
+// network over (ordered code, original index) pairs, one per lane.  The index makes every
+// pair distinct, so the network's result is the stable order (equal codes keep their input
+// order); padding lanes carry the largest code and indices >= len, so they sort last.  Each
+// lane then takes its key and value from the lane that held the element (shuffles only: the
+// segment may be sorted in place).
+template <class K, class V, bool DESC>
+__device__ inline void seg_warp_bitonic(typename RadixKey<K>::B* gk, V* gv, V* gs, uint32_t len) {
+    typedef typename RadixKey<K>::B KB;
+    typedef typename RadixKey<K>::U U;
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool valid = lane < len;
+    const KB key = valid ? gk[lane] : KB(0);
+    const V val = valid ? gv[lane] : V();
+    U code = ~U(0);
+    if (valid) {
+        code = RadixKey<K>::ordered(key);
+        if (DESC) code = ~code;
+    }
+    uint32_t idx = lane;
+#pragma unroll
+    for (uint32_t k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const U oc = __shfl_xor_sync(0xffffffffu, code, (int)j);
+            const uint32_t oi = __shfl_xor_sync(0xffffffffu, idx, (int)j);
+            const bool other_less = oc < code || (oc == code && oi < idx);
+            // blocks of k alternate direction; the lower lane of a pair keeps the smaller
+            // element in an ascending block and the larger one in a descending block
+            const bool asc = (lane & k) == 0, lower = (lane & j) == 0;
+            if ((asc == lower) == other_less) { code = oc; idx = oi; }
+        }
+    }
+    const KB sk = shfl_any(key, (int)idx);
+    const V sv = shfl_any(val, (int)idx);
+    const V x = valid ? sv : V();
+    V incl = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const V y = shfl_up_any(incl, d);
+        if (lane >= (uint32_t)d) incl += y;
+    }
+    if (valid) {
+        gk[lane] = sk;
+        gv[lane] = sv;
+        if (gs) gs[lane] = incl - x;
+    }
+}
+
 template <class K, class V, int ITEMS>
 constexpr size_t seg_sort_scan_smem() {
     return (size_t)256 * ITEMS * (2 * sizeof(V) + sizeof(typename RadixKey<K>::B)) + 8 * 256 * 4;
@@ -264,7 +319,8 @@ __global__ void __launch_bounds__(256, MINB) seg_sort_scan_kernel(typename Radix
                                                                 V* __restrict__ tv, const OFF* __restrict__ off,
                                                                 const uint32_t* __restrict__ queue,
                                                                 unsigned long long nseg, SegCtrl* ctrl,
-                                                                const SegItem* __restrict__ items) {
+                                                                const SegItem* __restrict__ items,
+                                                                uint32_t warp_small) {
     typedef typename RadixKey<K>::B KB;
     constexpr int TILE = 256 * ITEMS;
     constexpr int D = RadixKey<K>::DIGITS;
@@ -452,6 +508,7 @@ __global__ void __launch_bounds__(256, MINB) seg_sort_scan_kernel(typename Radix
             unsigned long long wb;
             fetch(mine, wk, wv, ws, wl, wb);
             if (wl > WSEG) defer = mine;
+            else if (wl > 0 && wl <= warp_small) seg_warp_bitonic<K, V, DESC>(wk, wv, ws, wl);
             else if (wl > 0)
                 seg_warp_sort_scan<K, V, DESC, ITEMS>(wk, wv, ws, wl, s_k + warp * WSEG, s_v + warp * WSEG,
                                                       s_whist + warp * 256);

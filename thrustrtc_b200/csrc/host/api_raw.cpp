@@ -124,4 +124,16 @@ int trtc_raw_segmented_autotune(int key_type, const unsigned long long* offsets,
     return segmented_autotune(key_type, offsets, (size_t)nseg, (size_t)n, S(stream), &chosen) ? chosen : -1;
 }
 
+unsigned long long trtc_raw_segmented_tuning_json(char* out, unsigned long long cap) {
+    const std::string j = segmented_tuning_json();
+    if (out && cap) {
+        const size_t c = j.size() < cap - 1 ? j.size() : (size_t)cap - 1;
+        memcpy(out, j.data(), c);
+        out[c] = 0;
+    }
+    return j.size();
+}
+
+int trtc_raw_segmented_tuning_load(const char* json) { return segmented_tuning_load(json) ? 0 : -1; }
+
 }  // extern "C"

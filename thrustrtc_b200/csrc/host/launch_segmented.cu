@@ -1,8 +1,18 @@
 // launch_segmented.cu -- batched segmented sort + exclusive scan (one persistent launch over
-// all segments, fed by a device work queue), its workspace sizing, and the autotuner that
-// picks the tile configuration per key type from timed trial runs.
+// all segments, fed by a device work queue), its workspace sizing, and the tuning table of
+// size classes: per key type, the items per thread (which sets the one-warp and on-chip class
+// limits, 32 x ITEMS and 256 x ITEMS keys) and the limit of the counter-free warp class (0 or
+// 32 keys), picked by an autotuner from timed trial runs on the batch's own segment lengths and
+// kept as versioned JSON (compiled-in defaults until a table is loaded or tuned).  The digit
+// width is 8 bits in every radix class: on-chip ranking spends one ballot per key bit whatever
+// the width, so narrower digits only add scatter passes and wider ones outgrow a warp's
+// counters.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "../device/trtc_segmented.cuh"
@@ -15,9 +25,17 @@ using namespace trtc;
 
 namespace {
 
-constexpr int SEG_CONFIGS[] = {8, 16};  // items per thread: small-class limit 2048 or 4096 keys
+struct SegShape {
+    int items;       // items per thread: one-warp class <= 32 x items, on-chip class <= 256 x items
+    int warp_small;  // counter-free (bitonic) warp class limit: 0 (off) or 32 keys
+    float ms;        // trial time that chose it (0: compiled-in default or loaded)
+};
+constexpr SegShape SEG_DEFAULT = {16, 32, 0.f};
+constexpr SegShape SEG_CONFIGS[] = {{8, 0, 0.f}, {8, 32, 0.f}, {16, 0, 0.f}, {16, 32, 0.f}};
+constexpr int SEG_TUNING_VERSION = 1;
 std::mutex g_seg_mu;
-std::map<int, int> g_seg_items;  // key type -> tuned items per thread
+std::map<int, SegShape> g_seg_tuning;  // key type -> tuned shape
+bool g_seg_env_loaded = false;
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -35,7 +53,7 @@ size_t ws_bytes(size_t n, size_t nseg) {
 
 template <class K, bool DESC, int ITEMS>
 bool seg_run_cfg(void* keys, void* vals, void* scan, const unsigned long long* off, size_t nseg, size_t n, void* ws,
-                 cudaStream_t s) {
+                 uint32_t warp_small, cudaStream_t s) {
     typedef typename RadixKey<K>::B KB;
     typedef uint32_t V;
     unsigned char* p = (unsigned char*)ws;
@@ -77,7 +95,8 @@ bool seg_run_cfg(void* keys, void* vals, void* scan, const unsigned long long* o
     }
     size_t grid = (size_t)per_sm * sms;
     if (grid > nseg) grid = nseg;
-    kernel<<<(unsigned)grid, 256, smem, s>>>((KB*)keys, (V*)vals, (V*)scan, tk, tv, off, queue, nseg, ctrl, nullptr);
+    kernel<<<(unsigned)grid, 256, smem, s>>>((KB*)keys, (V*)vals, (V*)scan, tk, tv, off, queue, nseg, ctrl, nullptr,
+                                             warp_small);
     ktimer_mark("seg_sort_scan_kernel", s);
     count_launch(2);
     if constexpr (is_float_key<K>()) {
@@ -90,29 +109,109 @@ bool seg_run_cfg(void* keys, void* vals, void* scan, const unsigned long long* o
 }
 
 template <class K, bool DESC>
-bool seg_run(int items, void* keys, void* vals, void* scan, const unsigned long long* off, size_t nseg, size_t n,
-             void* ws, cudaStream_t s) {
-    if (items == 16) return seg_run_cfg<K, DESC, 16>(keys, vals, scan, off, nseg, n, ws, s);
-    return seg_run_cfg<K, DESC, 8>(keys, vals, scan, off, nseg, n, ws, s);
+bool seg_run(const SegShape& sh, void* keys, void* vals, void* scan, const unsigned long long* off, size_t nseg,
+             size_t n, void* ws, cudaStream_t s) {
+    const uint32_t ws_small = (uint32_t)sh.warp_small;
+    if (sh.items == 16) return seg_run_cfg<K, DESC, 16>(keys, vals, scan, off, nseg, n, ws, ws_small, s);
+    return seg_run_cfg<K, DESC, 8>(keys, vals, scan, off, nseg, n, ws, ws_small, s);
 }
 
 template <class K>
-bool seg_dispatch_desc(int items, bool desc, void* keys, void* vals, void* scan, const unsigned long long* off,
-                       size_t nseg, size_t n, void* ws, cudaStream_t s) {
-    return desc ? seg_run<K, true>(items, keys, vals, scan, off, nseg, n, ws, s)
-                : seg_run<K, false>(items, keys, vals, scan, off, nseg, n, ws, s);
+bool seg_dispatch_desc(const SegShape& sh, bool desc, void* keys, void* vals, void* scan,
+                       const unsigned long long* off, size_t nseg, size_t n, void* ws, cudaStream_t s) {
+    return desc ? seg_run<K, true>(sh, keys, vals, scan, off, nseg, n, ws, s)
+                : seg_run<K, false>(sh, keys, vals, scan, off, nseg, n, ws, s);
 }
 
-bool seg_dispatch(int tc, int items, bool desc, void* keys, void* vals, void* scan, const unsigned long long* off,
-                  size_t nseg, size_t n, void* ws, cudaStream_t s) {
+bool seg_dispatch(int tc, const SegShape& sh, bool desc, void* keys, void* vals, void* scan,
+                  const unsigned long long* off, size_t nseg, size_t n, void* ws, cudaStream_t s) {
     switch (tc) {
-        case TC_U32: return seg_dispatch_desc<uint32_t>(items, desc, keys, vals, scan, off, nseg, n, ws, s);
-        case TC_I32: return seg_dispatch_desc<int32_t>(items, desc, keys, vals, scan, off, nseg, n, ws, s);
-        case TC_F32: return seg_dispatch_desc<float>(items, desc, keys, vals, scan, off, nseg, n, ws, s);
-        case TC_U64: return seg_dispatch_desc<uint64_t>(items, desc, keys, vals, scan, off, nseg, n, ws, s);
-        case TC_I64: return seg_dispatch_desc<int64_t>(items, desc, keys, vals, scan, off, nseg, n, ws, s);
+        case TC_U32: return seg_dispatch_desc<uint32_t>(sh, desc, keys, vals, scan, off, nseg, n, ws, s);
+        case TC_I32: return seg_dispatch_desc<int32_t>(sh, desc, keys, vals, scan, off, nseg, n, ws, s);
+        case TC_F32: return seg_dispatch_desc<float>(sh, desc, keys, vals, scan, off, nseg, n, ws, s);
+        case TC_U64: return seg_dispatch_desc<uint64_t>(sh, desc, keys, vals, scan, off, nseg, n, ws, s);
+        case TC_I64: return seg_dispatch_desc<int64_t>(sh, desc, keys, vals, scan, off, nseg, n, ws, s);
         default: set_error("segmented_sort_scan: key type must be int32, uint32, float, int64 or uint64"); return false;
     }
+}
+
+bool valid_shape(const SegShape& sh) { return (sh.items == 8 || sh.items == 16) && (sh.warp_small == 0 || sh.warp_small == 32); }
+
+// The table as JSON: {"format": ..., "version": 1, "digit_bits": 8, "entries": [{"key_type":
+// 5, "items": 16, "warp_small": 32, "ms": 3.1}, ...]}
+std::string tuning_json_locked() {
+    std::string j = "{\"format\": \"thrustrtc_b200.segmented_tuning\", \"version\": " +
+                    std::to_string(SEG_TUNING_VERSION) +
+                    ", \"classes\": [\"warp_bitonic: len <= warp_small\", \"warp_radix: len <= 32*items\", "
+                    "\"cta_onchip: len <= 256*items\", \"cta_global\"], \"digit_bits\": 8, \"entries\": [";
+    bool first = true;
+    for (const auto& kv : g_seg_tuning) {
+        char buf[160];
+        snprintf(buf, sizeof(buf), "%s{\"key_type\": %d, \"items\": %d, \"warp_small\": %d, \"ms\": %.4f}",
+                 first ? "" : ", ", kv.first, kv.second.items, kv.second.warp_small, kv.second.ms);
+        j += buf;
+        first = false;
+    }
+    return j + "]}";
+}
+
+// Reads the entries of a table written by tuning_json_locked (tolerant of whitespace and key
+// order inside an entry); rejects another format or version.
+bool tuning_load_locked(const char* json) {
+    const char* f = strstr(json, "\"thrustrtc_b200.segmented_tuning\"");
+    const char* v = strstr(json, "\"version\"");
+    if (!f || !v) { set_error("segmented tuning: not a thrustrtc_b200 segmented tuning table"); return false; }
+    v = strchr(v, ':');
+    if (!v || atoi(v + 1) != SEG_TUNING_VERSION) { set_error("segmented tuning: unsupported table version"); return false; }
+    auto field = [](const char* b, const char* e, const char* name, int* out) {
+        const char* p = strstr(b, name);
+        if (!p || p > e) return false;
+        p = strchr(p, ':');
+        if (!p || p > e) return false;
+        *out = atoi(p + 1);
+        return true;
+    };
+    std::map<int, SegShape> t;
+    const char* p = strstr(json, "\"entries\"");
+    while (p && (p = strchr(p, '{')) != nullptr) {
+        const char* e = strchr(p, '}');
+        if (!e) break;
+        int kt = 0, it = 0, wsm = 0;
+        if (!field(p, e, "\"key_type\"", &kt) || !field(p, e, "\"items\"", &it) ||
+            !field(p, e, "\"warp_small\"", &wsm)) {
+            set_error("segmented tuning: malformed entry");
+            return false;
+        }
+        SegShape sh{it, wsm, 0.f};
+        if (!valid_shape(sh)) { set_error("segmented tuning: unsupported shape in the table"); return false; }
+        t[kt] = sh;
+        p = e + 1;
+    }
+    for (const auto& kv : t) g_seg_tuning[kv.first] = kv.second;
+    return true;
+}
+
+// TRTC_SEG_TUNING_FILE: a table to load at the first batched call of the process
+void load_env_tuning_locked() {
+    if (g_seg_env_loaded) return;
+    g_seg_env_loaded = true;
+    const char* path = getenv("TRTC_SEG_TUNING_FILE");
+    if (!path || !*path) return;
+    FILE* fp = fopen(path, "rb");
+    if (!fp) return;
+    std::string text;
+    char buf[4096];
+    size_t r;
+    while ((r = fread(buf, 1, sizeof(buf), fp)) > 0) text.append(buf, r);
+    fclose(fp);
+    tuning_load_locked(text.c_str());
+}
+
+SegShape tuned_shape(int tc) {
+    std::lock_guard<std::mutex> lk(g_seg_mu);
+    load_env_tuning_locked();
+    auto it = g_seg_tuning.find(tc);
+    return it == g_seg_tuning.end() ? SEG_DEFAULT : it->second;
 }
 
 __global__ void seg_fill_kernel(uint32_t* k, uint32_t* v, size_t words, unsigned long long seed) {
@@ -133,10 +232,19 @@ size_t segmented_workspace_bytes(int tc, size_t n, size_t nseg) {
     return (tc == TC_U64 || tc == TC_I64) ? ws_bytes<uint64_t>(n, nseg) : ws_bytes<uint32_t>(n, nseg);
 }
 
-int segmented_tuned_items(int tc) {
+int segmented_tuned_items(int tc) { return tuned_shape(tc).items; }
+
+std::string segmented_tuning_json() {
     std::lock_guard<std::mutex> lk(g_seg_mu);
-    auto it = g_seg_items.find(tc);
-    return it == g_seg_items.end() ? 16 : it->second;
+    load_env_tuning_locked();
+    return tuning_json_locked();
+}
+
+bool segmented_tuning_load(const char* json) {
+    if (!json) { set_error("segmented tuning: no table"); return false; }
+    std::lock_guard<std::mutex> lk(g_seg_mu);
+    g_seg_env_loaded = true;
+    return tuning_load_locked(json);
 }
 
 bool segmented_sort_scan_raw(int tc, void* keys, void* vals, void* scan, const unsigned long long* off, size_t nseg,
@@ -148,7 +256,7 @@ bool segmented_sort_scan_raw(int tc, void* keys, void* vals, void* scan, const u
         set_error("segmented_sort_scan: workspace too small (see trtc_raw_segmented_workspace_bytes)");
         return false;
     }
-    return seg_dispatch(tc, segmented_tuned_items(tc), desc, keys, vals, scan, off, nseg, n, ws, s);
+    return seg_dispatch(tc, tuned_shape(tc), desc, keys, vals, scan, off, nseg, n, ws, s);
 }
 
 // Times every configuration on a copy of the batch shape (random keys, the caller's segment
@@ -156,6 +264,10 @@ bool segmented_sort_scan_raw(int tc, void* keys, void* vals, void* scan, const u
 bool segmented_autotune(int tc, const unsigned long long* off, size_t nseg, size_t n, cudaStream_t s, int* chosen) {
     if (!ensure_device()) return false;
     if (nseg == 0 || n == 0) { *chosen = segmented_tuned_items(tc); return true; }
+    if (tc != TC_U32 && tc != TC_I32 && tc != TC_F32 && tc != TC_U64 && tc != TC_I64) {
+        set_error("segmented autotune: key type must be int32, uint32, float, int64 or uint64");
+        return false;
+    }
     const size_t ksz = (tc == TC_U64 || tc == TC_I64) ? 8 : 4;
     const size_t wsb = segmented_workspace_bytes(tc, n, nseg);
     void *k = nullptr, *v = nullptr, *sc = nullptr, *ws = nullptr;
@@ -163,9 +275,9 @@ bool segmented_autotune(int tc, const unsigned long long* off, size_t nseg, size
               TRTC_CUDA(cudaMalloc(&sc, n * 4)) && TRTC_CUDA(cudaMalloc(&ws, wsb));
     cudaEvent_t a = nullptr, b = nullptr;
     ok = ok && TRTC_CUDA(cudaEventCreate(&a)) && TRTC_CUDA(cudaEventCreate(&b));
-    int best = 16;
+    SegShape best = SEG_DEFAULT;
     float best_ms = 1e30f;
-    for (int cfg : SEG_CONFIGS) {
+    for (const SegShape& cfg : SEG_CONFIGS) {
         if (!ok) break;
         float tot = 0.f;
         for (int rep = 0; ok && rep < 4; rep++) {
@@ -176,7 +288,7 @@ bool segmented_autotune(int tc, const unsigned long long* off, size_t nseg, size
             float ms = 0.f;
             if (ok && rep > 0 && TRTC_CUDA(cudaEventElapsedTime(&ms, a, b))) tot += ms;
         }
-        if (ok && tot < best_ms) { best_ms = tot; best = cfg; }
+        if (ok && tot < best_ms) { best_ms = tot; best = cfg; best.ms = tot / 3.f; }
     }
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
@@ -184,9 +296,10 @@ bool segmented_autotune(int tc, const unsigned long long* off, size_t nseg, size
     if (!ok) return false;
     {
         std::lock_guard<std::mutex> lk(g_seg_mu);
-        g_seg_items[tc] = best;
+        g_seg_env_loaded = true;
+        g_seg_tuning[tc] = best;
     }
-    *chosen = best;
+    *chosen = best.items;
     return true;
 }
 

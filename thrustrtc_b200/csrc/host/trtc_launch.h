@@ -1,5 +1,6 @@
 // trtc_launch.h -- entry points of the nvcc-built (built-in type / operator) kernels.
 #pragma once
+#include <string>
 #include <cstddef>
 #include <cuda_runtime.h>
 
@@ -35,5 +36,7 @@ int segmented_tuned_items(int tc);
 bool segmented_sort_scan_raw(int tc, void* keys, void* vals, void* scan, const unsigned long long* off, size_t nseg,
                              size_t n, void* ws, size_t ws_bytes, bool desc, cudaStream_t s);
 bool segmented_autotune(int tc, const unsigned long long* off, size_t nseg, size_t n, cudaStream_t s, int* chosen);
+std::string segmented_tuning_json();
+bool segmented_tuning_load(const char* json);
 
 }  // namespace trtc_host

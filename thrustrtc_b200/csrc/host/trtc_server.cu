@@ -363,7 +363,7 @@ private:
             count_launch();
         }
         kernel<<<grid, 256, smem, s>>>(nullptr, nullptr, nullptr, (KB*)tk, (uint32_t*)tv, nullptr, nullptr, g, ctrl,
-                                       items);
+                                       items, 32u);
         count_launch();
         if constexpr (FK) {
             seg_rotate_kernel<K, uint32_t, unsigned long long, false><<<grid, 256, 0, s>>>(
