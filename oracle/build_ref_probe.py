@@ -7,9 +7,8 @@ tree, together with a small driver written here, into ``oracle/_ref/ref_probe`` 
 on a fixed list of edge values.  The printed results become tests/golden/builtin_h_probe.json
 (via tests/golden/make_golden.py), which the CPU tests compare the oracle against.
 
-Nothing else of the reference is buildable this way: its kernels are NVRTC strings that
-need a GPU, libcuda, a generated header (internal/pack_headers.cpp) and the unqlite
-submodule, which is empty.  Test infrastructure only.
+The whole reference library is built by oracle/build_ref.py (its kernels then run on a GPU
+through NVRTC); this probe needs no GPU.  Test infrastructure only.
 """
 import json
 import os
@@ -18,7 +17,10 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
-REF_ROOT = os.environ.get("TRTC_REFERENCE_ROOT", "/root/reference")
+sys.path.insert(0, os.path.dirname(HERE))
+from oracle.build_ref import ref_root  # noqa: E402  (the reference tree this recipe reads)
+
+REF_ROOT = ref_root()
 
 DRIVER = r"""
 #include <cstdint>

@@ -60,7 +60,10 @@ def glibc_shuffles():
     return a, keys, vals
 
 
-REF_ROOT = os.environ.get("TRTC_REFERENCE_ROOT", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.build_ref import ref_root  # noqa: E402  (the reference tree this script reads)
+
+REF_ROOT = ref_root()
 
 
 def api_h_exports():
