@@ -646,6 +646,15 @@ def _seg_sigs(L):
     L.trtc_raw_segmented_autotune.restype = ctypes.c_int
     L.trtc_raw_segmented_autotune.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_ulonglong,
                                               ctypes.c_ulonglong, ctypes.c_void_p]
+    L.trtc_raw_segmented_tuning_json.restype = ctypes.c_ulonglong
+    L.trtc_raw_segmented_tuning_json.argtypes = [ctypes.c_char_p, ctypes.c_ulonglong]
+
+
+def _seg_tuning(L):
+    """The batched kernel's size-class table (versioned JSON), parsed."""
+    buf = ctypes.create_string_buffer(8192)
+    L.trtc_raw_segmented_tuning_json(buf, 8192)
+    return json.loads(buf.value.decode())
 
 
 def run_segmented(args):
@@ -832,7 +841,8 @@ def run_segmented(args):
                            "keys": "uint32 uniform", "values": "uint32 = index",
                            "op": "stable sort by key per segment, then exclusive Plus scan of its values",
                            "launch": "1 persistent launch from a device work queue (+1 queue kernel), CUDA graph replay",
-                           "autotuned_items_per_thread": items, "parallelism": "replicas x%d" % world,
+                           "autotuned_items_per_thread": items, "tuning_table": _seg_tuning(L),
+                           "parallelism": "replicas x%d" % world,
                            "l2": "inputs (%d MiB) exceed the 126 MB L2" % (8 * n >> 20)},
                 "roofline": {"bound": "hbm", "kernel": "seg_sort_scan_kernel", "achieved": achieved, "peak": peak,
                              "peak_source": peak_src, "unit": "GB/s",
