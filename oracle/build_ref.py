@@ -17,8 +17,12 @@ read):
   (``internal/impl_context.inl:404-648``); this stub makes every one of them fail, so every
   kernel is compiled by NVRTC in-process (warm up once per process before timing);
 * compiles every library and Python-binding source that ``python/CMakeLists.txt`` lists,
-  where it lies, with ``g++ -std=c++17 -fPIC -include cstdio`` (``internal/launch_calc.cpp``
-  calls printf without including <cstdio>), into ``_ref/ThrustRTC/libPyThrustRTC.so``;
+  where it lies, with ``g++ -std=c++17 -fPIC -include cstdio`` (some sources call printf
+  without including <cstdio>), into ``_ref/ThrustRTC/libPyThrustRTC.so`` -- except
+  ``internal/launch_calc.cpp``, whose vendored occupancy calculator knows compute
+  capabilities up to 8.x only: on a B200 it leaves every block size at -1 and every launch of
+  the reference fails without a message.  ``oracle/ref_launch_calc.cpp`` (written here)
+  answers the same two queries through the driver's occupancy API instead;
 * places the reference's unmodified Python package (``python/ThrustRTC/*.py``) beside that
   library, where its ``Native.py:9-12`` looks for it, and copies the reference's hot-path
   Python test programs to ``_ref/python_test/`` (run on the GPU box, they produce golden
@@ -46,7 +50,7 @@ OUT = os.path.join(HERE, "_ref")
 DEFAULT_REF = "/root/reference"
 
 LIB_SOURCES = """
-thirdparty/crc64/crc64.cpp internal/launch_calc.cpp internal/cuda_wrapper.cpp internal/nvtrc_wrapper.cpp
+thirdparty/crc64/crc64.cpp internal/cuda_wrapper.cpp internal/nvtrc_wrapper.cpp
 internal/general_reduce.cpp internal/general_scan.cpp internal/general_scan_by_key.cpp internal/general_copy_if.cpp
 internal/general_find.cpp internal/merge_sort.cpp internal/radix_sort.cpp TRTCContext.cpp DVVector.cpp DVTuple.cpp
 fake_vectors/DVRange.cpp fake_vectors/DVConstant.cpp fake_vectors/DVCounter.cpp fake_vectors/DVDiscard.cpp
@@ -59,7 +63,7 @@ python/api_utils.cpp python/api_Context.cpp python/api_DeviceViewable.cpp python
 python/api_DVTuple.cpp python/api_FakeVectors.cpp python/api_Functor.cpp python/api_Transformations.cpp
 python/api_Copying.cpp python/api_Reductions.cpp python/api_PrefixSums.cpp python/api_Reordering.cpp
 python/api_Searching.cpp python/api_Merging.cpp python/api_Sorting.cpp
-""".split()
+""".split() + [os.path.join(HERE, "ref_launch_calc.cpp")]  # in place of internal/launch_calc.cpp
 
 # the reference's hot-path Python test programs (printouts become golden files)
 PY_TESTS = ["test_sort.py", "test_scan.py", "test_transform_scan.py", "test_scan_by_key.py", "test_copy.py",
