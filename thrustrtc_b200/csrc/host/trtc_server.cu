@@ -226,14 +226,19 @@ private:
                 temp += r.temp;
             }
         }
-        // remove the group from the queue
-        std::deque<long long> rest;
-        size_t gi = 0;
-        for (long long id : queue_) {
-            if (gi < group.size() && id == group[gi]) { gi++; continue; }
-            rest.push_back(id);
+        // remove the group from the queue (the head alone: O(1), so a long backlog of plain
+        // requests costs no host time per launch)
+        if (group.size() == 1) {
+            queue_.pop_front();
+        } else {
+            std::deque<long long> rest;
+            size_t gi = 0;
+            for (long long id : queue_) {
+                if (gi < group.size() && id == group[gi]) { gi++; continue; }
+                rest.push_back(id);
+            }
+            queue_.swap(rest);
         }
-        queue_.swap(rest);
         sl.ids = group;
         sl.temp = temp;
         used_ += temp;
