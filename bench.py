@@ -1088,7 +1088,7 @@ def run_serving(args):
     dev = torch.device("cuda", local)
     count = args.n or WORKLOADS["serving_c5"][0]
     levels = tuple(float(f) for f in args.levels.split(",")) if args.levels else SERVING_GRID
-    rec = _serving_measure(count, dev, shared_grid=True, grid=levels)
+    rec = _serving_measure(count, dev, shared_grid=True, grid=levels, coalesce=args.coalesce, streams=args.streams)
     line = {"metric": WORKLOADS["serving_c5"][4], "value": rec["capacity_rps"]["served"], "unit": "requests/s",
             "n_gpus": 1, "steps": len(rec["levels"]), "warmup": 1,
             "ms_per_step": 1e3 * 1000 / rec["capacity_rps"]["served"], "higher_is_better": True,
@@ -1101,7 +1101,7 @@ def run_serving(args):
     return 0
 
 
-def _serving_measure(count, dev, shared_grid=True, grid=SERVING_GRID, block=1000):
+def _serving_measure(count, dev, shared_grid=True, grid=SERVING_GRID, block=1000, coalesce=1 << 16, streams=8):
     """Poisson arrivals of `count` mixed requests into the request server (continuous
     batching: 8 streams, coalescing of requests up to 2^16 elements, 32 GB admission budget)
     beside the plain path (the same requests one call at a time on one stream, no coalescing).
@@ -1216,7 +1216,7 @@ def _serving_measure(count, dev, shared_grid=True, grid=SERVING_GRID, block=1000
                 "p99_ms": float(np.percentile(lat, 99) * 1e3)}
 
     budget = 32 << 30
-    served = L.trtc_server_create(budget, 8, 1 << 16)
+    served = L.trtc_server_create(budget, streams, coalesce)
     plain = L.trtc_server_create(budget, 1, 0)
     if not served or not plain:
         raise RuntimeError(N.last_error())
@@ -1249,7 +1249,8 @@ def _serving_measure(count, dev, shared_grid=True, grid=SERVING_GRID, block=1000
                        "mix": "60% Sort_By_Key (+uint32 values), 25% exclusive scan, 15% reduce",
                        "sizes": "log-uniform 2^10..2^24", "types": "uint32 / int64 / float equal shares",
                        "elements": elems, "budget_bytes": budget,
-                       "server": "8 streams, coalescing up to 2^16 elements per request, admission by budget",
+                       "server": "%d streams, coalescing of requests up to %d elements, admission by budget"
+                                 % (streams, coalesce),
                        "plain": "same requests, one call at a time on one stream, no coalescing",
                        "grid": ("the same offered rates for both paths, as fractions of the plain path's "
                                 "capacity") if shared_grid else "fractions of each path's own capacity",
@@ -1273,6 +1274,8 @@ def main():
     ap.add_argument("--no-sub", action="store_true", help="default run: skip the scan / reduce / serving records")
     ap.add_argument("--sub-requests", type=int, default=1000, help="requests of the serving record")
     ap.add_argument("--levels", default="", help="serving_c5: comma-separated fractions of the plain capacity")
+    ap.add_argument("--coalesce", type=int, default=1 << 16, help="serving_c5: largest request the server coalesces")
+    ap.add_argument("--streams", type=int, default=8, help="serving_c5: streams of the server")
     args = ap.parse_args()
     _, world, _ = dist_env()
     if args.gpus != world and not (args.gpus == 1 and world == 1):
