@@ -40,9 +40,21 @@ template <> inline uint32_t d_u32<float>(float v) {
     return u;
 }
 template <class T> inline uint64_t d_u64(T v) { return (uint64_t)v; }
+// built_in.h:450-457 as the reference runs it on the GPU (NVRTC-compiled; recorded by
+// tests/golden/make_ref_fixtures.py in tests/golden/ref_keymap_probe.json): negative
+// finite values and -0.0 map to 0 - |bits| as the source reads, but a negative NaN maps to
+// (0 - |bits|) with bit 63 clear, its signalling payload first quietened (bit 51 set) -- so
+// -NaN orders just above +0.0.  The same source compiled for the CPU keeps bit 63
+// (tests/golden/builtin_h_probe.json); the sort follows the GPU.
 template <> inline uint64_t d_u64<double>(double v) {
     uint64_t u; std::memcpy(&u, &v, 8);
-    if (u & 0x8000000000000000ull) u = 0ull - (u & 0x7FFFFFFFFFFFFFFFull);
+    if (u & 0x8000000000000000ull) {
+        uint64_t mag = u & 0x7FFFFFFFFFFFFFFFull;
+        const bool nan = mag > 0x7FF0000000000000ull;
+        if (nan) mag |= 0x0008000000000000ull;
+        u = 0ull - mag;
+        if (nan) u &= 0x7FFFFFFFFFFFFFFFull;
+    }
     return u;
 }
 

@@ -8,6 +8,8 @@ library's kernels to what the reference itself computes.
 writes, under DIR:
 * ``ref_fixtures.npz``: every case of tests/golden/ref_cases.py (inputs and the reference's
   outputs), run through the reference's own, unmodified Python package;
+* ``ref_keymap_probe.json``: the reference's key maps (d_u64 / d_u32) evaluated on the GPU on
+  the edge bit patterns of ref_cases, and those patterns after the reference's TRTC_Copy;
 * ``ref_printouts.json``: the stdout of the reference's hot-path Python test programs
   (python/test/*.py, copied to oracle/_ref/python_test by the build recipe), run against
   the reference's library, and ``ours_printouts.json`` against this repository's library
@@ -59,6 +61,31 @@ def worker_fixtures(out):
     res = ref_cases.run_all(T)
     np.savez_compressed(os.path.join(out, "ref_fixtures.npz"), **ref_cases.pack(res))
     print("fixtures: %d arrays" % len(res))
+
+
+def worker_probe(out):
+    """The reference's key maps evaluated on the GPU (d_u64 / d_u32 of built_in.h, called from a
+    TRTC_For kernel) on the edge bit patterns of ref_cases, and the same patterns after the
+    reference's TRTC_Copy: the key the reference's radix sort actually orders by."""
+    import numpy as np
+    import ThrustRTC as T
+    sys.path.insert(0, HERE)
+    import ref_cases
+    res = {}
+    for tag, dt, bdt, pats, fn, cls in (("f64", np.float64, np.uint64, ref_cases.F64_EDGE, "d_u64", "uint64_t"),
+                                        ("f32", np.float32, np.uint32, ref_cases.F32_EDGE, "d_u32", "uint32_t")):
+        bits = np.array(pats, dtype=bdt)
+        dk = T.device_vector_from_numpy(bits.view(dt))
+        dmap = T.device_vector(cls, len(bits))
+        T.For(["vin", "vout"], "idx", "        vout[idx] = %s(vin[idx]);\n" % fn).launch_n(len(bits), [dk, dmap])
+        dcp = T.device_vector("double" if tag == "f64" else "float", len(bits))
+        T.Copy(dk, dcp)
+        copied = dcp.to_host().view(bdt)
+        res[tag] = [{"bits": hex(int(b)), "key": hex(int(m)), "after_copy": hex(int(c))}
+                    for b, m, c in zip(bits, dmap.to_host(), copied)]
+    with open(os.path.join(out, "ref_keymap_probe.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    print("probe:", len(res["f64"]), "f64 and", len(res["f32"]), "f32 patterns")
 
 
 def printouts(out):
@@ -150,12 +177,15 @@ if __name__ == "__main__":
     os.makedirs(a.out, exist_ok=True)
     if a.worker == "fixtures":
         worker_fixtures(a.out)
+    elif a.worker == "probe":
+        worker_probe(a.out)
     elif a.worker == "timing":
         worker_timing(a.out)
     else:
         if not (a.fixtures or a.printouts or a.timing):
             a.fixtures = a.printouts = True
         if a.fixtures:
+            _child("probe", a.out)
             _child("fixtures", a.out)
         if a.printouts:
             printouts(a.out)

@@ -21,7 +21,7 @@ class Vec:
         self.a = a
 
     def to_host(self, begin=0, end=-1):
-        return self.a[begin:] if end == -1 else self.a[begin:end].copy()
+        return (self.a[begin:] if end == -1 else self.a[begin:end]).copy()
 
 
 def device_vector_from_numpy(a):

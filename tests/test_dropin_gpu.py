@@ -28,6 +28,14 @@ def _programs():
     return sorted(json.load(open(GOLD)))
 
 
+# Lines where this library prints the documented result and the reference does not: the
+# reference's C ABI passes values_in as the keys output of Unique_By_Key_Copy
+# (python/api_Reordering.cpp:120), so over its own library test_unique.py prints the untouched
+# keys_out ([0 0 0 0]) and a values_out read while values_in was being overwritten.  This
+# library writes keys_out, as the reference's C++ TRTC_Unique_By_Key_Copy does (unique.cpp:56-72).
+EXPECTED_DEVIATIONS = {"test_unique.py": {8: "[1 3 2 1]", 9: "[9 8 5 3]", 10: "[1 3 2 1]", 11: "[9 8 5 3]"}}
+
+
 @pytest.mark.parametrize("prog", _programs())
 def test_reference_program_prints_the_same(cuda, prog):
     gold = json.load(open(GOLD))[prog]
@@ -40,4 +48,8 @@ def test_reference_program_prints_the_same(cuda, prog):
     r = subprocess.run([sys.executable, os.path.join(PROGS, prog)], env=env, cwd=PROGS, capture_output=True,
                        text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
-    assert r.stdout == gold["stdout"]
+    got, want = r.stdout.splitlines(), gold["stdout"].splitlines()
+    assert len(got) == len(want)
+    dev = EXPECTED_DEVIATIONS.get(prog, {})
+    for i, (g, w) in enumerate(zip(got, want)):
+        assert g == (dev[i] if i in dev else w), (i, g, w)

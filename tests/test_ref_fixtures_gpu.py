@@ -27,3 +27,11 @@ def test_library_matches_reference_outputs(cuda):
     res = ref_cases.run_all(T)
     bad = ref_cases.compare(fix, res)
     assert not bad, bad
+    # where the reference's C ABI deviates from its own C++ API (ref_cases.ABI_DEVIATIONS), this
+    # library gives the C++ API's result, which the oracle restates
+    sys.path.insert(0, HERE)
+    import oracle_api
+    want = ref_cases.run_all(oracle_api)
+    for k in want:
+        if k.startswith(ref_cases.ABI_DEVIATIONS):
+            assert np.asarray(res[k]).tobytes() == np.asarray(want[k]).tobytes(), k

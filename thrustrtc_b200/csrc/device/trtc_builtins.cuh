@@ -157,9 +157,17 @@ template <> __device__ inline uint32_t d_u32<float>(float v) {
     return u;
 }
 template <typename T> __device__ inline uint64_t d_u64(T v) { return (uint64_t)v; }
+// as the reference's d_u64<double> evaluates on the GPU: a negative NaN (quietened) maps to
+// 0 - |bits| with bit 63 clear
 template <> __device__ inline uint64_t d_u64<double>(double v) {
     uint64_t u = (uint64_t)__double_as_longlong(v);
-    if (u & 0x8000000000000000ull) u = 0ull - (u & 0x7FFFFFFFFFFFFFFFull);
+    if (u & 0x8000000000000000ull) {
+        uint64_t mag = u & 0x7FFFFFFFFFFFFFFFull;
+        const bool nan = mag > 0x7FF0000000000000ull;
+        if (nan) mag |= 0x0008000000000000ull;
+        u = 0ull - mag;
+        if (nan) u &= 0x7FFFFFFFFFFFFFFFull;
+    }
     return u;
 }
 

@@ -187,10 +187,20 @@ template <> struct RadixKey<float> {
     static TRTC_FORCEINLINE bool is_nan(B u) { return (u & 0x7FFFFFFFu) > 0x7F800000u; }
     static TRTC_FORCEINLINE float value(B b) { return __uint_as_float(b); }
 };
+// double: d_u64 as the reference computes it on the GPU (built_in.h:450-457, compiled by
+// NVRTC): a negative NaN's code is 0 - |bits| with bit 63 clear, after its signalling payload
+// is quietened (bit 51 set), which orders it just above +0.0; every other value maps as the
+// source reads.
 template <> struct RadixKey<double> {
     typedef unsigned long long B; typedef unsigned long long U; enum { DIGITS = 8 };
     static TRTC_FORCEINLINE U ordered(B u) {
-        if (u & 0x8000000000000000ull) u = 0ull - (u & 0x7FFFFFFFFFFFFFFFull);
+        if (u & 0x8000000000000000ull) {
+            unsigned long long mag = u & 0x7FFFFFFFFFFFFFFFull;
+            const bool nan = mag > 0x7FF0000000000000ull;
+            if (nan) mag |= 0x0008000000000000ull;
+            u = 0ull - mag;
+            if (nan) u &= 0x7FFFFFFFFFFFFFFFull;
+        }
         return u ^ 0x8000000000000000ull;
     }
     static TRTC_FORCEINLINE bool is_nan(B u) { return (u & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull; }
