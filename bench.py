@@ -315,10 +315,80 @@ def run_reference(args):
             "data": "synthetic (SplitMix64 seed 0)", "config": _config(wl, n, world),
             "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference (fynv/ThrustRTC) has no CPU path and does not build in this image; "
-                    "the arm times the oracle's host restatement of its algorithm"}
+            "note": "the reference (fynv/ThrustRTC) has no CPU path (every kernel is an NVRTC string run on "
+                    "the GPU); the arm times the oracle's host restatement of its algorithm on the host cores",
+            "thrustrtc_same_gpu": _thrustrtc_gpu(wl, n)}
     print(json.dumps(line), flush=True)
     return 0
+
+
+# The reference itself on this box's GPU, for the record beside the host arm: its library as
+# built from its sources by oracle/build_ref.py (present when the repository was built where
+# the reference tree is), run through its own Python package in a child process.
+_REF_CALLS = {
+    "sort_by_key_u32": "T.Sort_By_Key(a[0], a[1])",
+    "inclusive_scan_i32": "T.Inclusive_Scan(a[0], a[1])",
+    "reduce_f32": "T.Reduce(a[0])",
+}
+
+
+def _thrustrtc_gpu(wl, n):
+    if wl not in _REF_CALLS:
+        return {"skipped": "timed for the plain sort, scan and reduce workloads only"}
+    try:
+        from oracle import build_ref
+    except ImportError as e:
+        return {"unavailable": "oracle/build_ref.py not importable: %s" % e}
+    pkg = build_ref.package_dir(False)
+    if pkg is None:
+        return {"unavailable": "oracle/_ref was not built (the reference tree was absent where the repository was built)"}
+    env = dict(os.environ)
+    cl = build_ref.cuda_lib_dir()
+    if cl:
+        env["LD_LIBRARY_PATH"] = cl + (":" + env["LD_LIBRARY_PATH"] if env.get("LD_LIBRARY_PATH") else "")
+    env["PYTHONPATH"] = pkg + ":" + ROOT + (":" + env["PYTHONPATH"] if env.get("PYTHONPATH") else "")
+    import subprocess
+    try:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--thrustrtc-child", wl, "--n", str(n)],
+                           env=env, capture_output=True, text=True, timeout=600)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "the reference's run exceeded 600 s"}
+    ls = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not ls:
+        return {"unavailable": "the reference's run failed (rc %d): %s" % (r.returncode, (r.stderr or r.stdout)[-300:])}
+    return json.loads(ls[-1])
+
+
+def _thrustrtc_child(wl, n):
+    """Times one call of the reference's own API on the workload's inputs, already on the
+    device: one warm-up call on a 4,096-element slice compiles its kernels (NVRTC), then three
+    calls, each bracketed by Wait() and timed by the host clock."""
+    import ThrustRTC as T
+    keys_h, vals_h = gen_inputs(wl, n)
+    def inputs(m):
+        if wl == "sort_by_key_u32":
+            return [T.device_vector_from_numpy(keys_h[:m]), T.device_vector_from_numpy(vals_h[:m])]
+        if wl == "inclusive_scan_i32":
+            return [T.device_vector_from_numpy(keys_h[:m]), T.device_vector("int32_t", m)]
+        return [T.device_vector_from_numpy(keys_h[:m])]
+    call = _REF_CALLS[wl]
+    a = inputs(4096)
+    eval(call)
+    T.Wait()
+    ts = []
+    for _ in range(3):
+        a = inputs(n) if wl == "sort_by_key_u32" or not ts else a
+        T.Wait()
+        t0 = time.perf_counter()
+        eval(call)
+        T.Wait()
+        ts.append(time.perf_counter() - t0)
+    best = min(ts)
+    print(json.dumps({"value": units_per_s_to_metric(wl, n, best), "unit": WORKLOADS[wl][5],
+                      "ms_per_call": best * 1e3, "ms_all_calls": [t * 1e3 for t in ts],
+                      "how": "the reference's library built from its sources (its block-size query answered by "
+                             "the CUDA driver, oracle/ref_launch_calc.cpp), its own Python package, inputs on "
+                             "the device, best of 3 calls after a warm-up compile; host clock with Wait()"}))
 
 
 def _dtype(wl):
@@ -1073,7 +1143,7 @@ def _srv_sigs(L):
     L.trtc_server_destroy.argtypes = [ctypes.c_void_p]
 
 
-SERVING_GRID = (0.25, 0.50, 0.75, 0.90, 1.00, 1.25, 1.50, 2.00, 2.50)
+SERVING_GRID = (0.25, 0.50, 0.75, 0.90, 1.00, 1.25, 1.50, 2.00, 2.50, 3.00, 3.50, 4.00)
 
 
 def run_serving(args):
@@ -1094,7 +1164,8 @@ def run_serving(args):
             "ms_per_step": 1e3 * 1000 / rec["capacity_rps"]["served"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32/i64/f32",
             "data": "synthetic (SplitMix64 seed 0 request mix; torch generator seed 0 contents)",
-            "config": rec["config"], "capacity_rps": rec["capacity_rps"], "levels": rec["levels"],
+            "config": rec["config"], "capacity_rps": rec["capacity_rps"], "sustained_rps": rec["sustained_rps"],
+            "levels": rec["levels"],
             "clocks": rec["clocks"], "gpu_launches": rec["gpu_launches"],
             "e2e": None, "cpu_baseline": None, "roofline": None}
     print(json.dumps(line), flush=True)
@@ -1240,7 +1311,12 @@ def _serving_measure(count, dev, shared_grid=True, grid=SERVING_GRID, block=1000
         L.trtc_server_destroy(plain)
     launches = N.launch_count() - lc0
     elems = sum(n for _, _, n in reqs)
+    # open-loop throughput: the highest request rate each path achieved under Poisson arrivals
+    sus_b = max(l["served"]["achieved_rps"] for l in levels)
+    sus_p = max(l["plain"]["achieved_rps"] for l in levels)
     return {"capacity_rps": {"served": cap_b, "plain": cap_p, "ratio": cap_b / cap_p},
+            "sustained_rps": {"served": sus_b, "plain": sus_p, "ratio": sus_b / sus_p,
+                              "how": "highest achieved rate over the offered-rate grid (Poisson arrivals)"},
             "levels": levels, "clocks": sampler.summary(), "gpu_launches": launches,
             "config": {"workload": "serving_c5", "requests": count, "block": block,
                        "sample": ("the full %d-request stream" % count) if count >= 200000 else
@@ -1276,7 +1352,11 @@ def main():
     ap.add_argument("--levels", default="", help="serving_c5: comma-separated fractions of the plain capacity")
     ap.add_argument("--coalesce", type=int, default=1 << 16, help="serving_c5: largest request the server coalesces")
     ap.add_argument("--streams", type=int, default=8, help="serving_c5: streams of the server")
+    ap.add_argument("--thrustrtc-child", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.thrustrtc_child:
+        _thrustrtc_child(args.thrustrtc_child, args.n or WORKLOADS[args.thrustrtc_child][0])
+        return 0
     _, world, _ = dist_env()
     if args.gpus != world and not (args.gpus == 1 and world == 1):
         if world == 1:
