@@ -94,6 +94,29 @@ def test_sort_by_key(N, name, vsize):
             assert gv.tobytes() == v[p].tobytes(), (name, n, vsize, desc)
 
 
+@pytest.mark.parametrize("name", ["uint32_t", "float", "int64_t"])
+@pytest.mark.parametrize("off", [0, 1, 2, 3])
+def test_sort_by_key_payload_offsets(N, name, off):
+    # 4-byte payloads of full tiles arrive by one bulk copy when the tile's payload address
+    # is 16-byte aligned, else by per-element copies; payload views at element offsets 0..3
+    # take both paths, and n leaves a partial last tile (per-element path) behind full ones
+    rng = np.random.default_rng(31 + off)
+    n = (1 << 20) + 4099
+    k = rand_keys(rng, name, n)
+    v = rng.integers(0, 2**32, n, dtype=np.uint32)
+    dk = dev(k)
+    vbuf = dev(np.concatenate([np.zeros(off, np.uint32), v]))
+    vp = ctypes.c_void_p(vbuf.data_ptr() + 4 * off)
+    rc = N.lib.trtc_raw_sort_by_key(N.TYPE_CODES[name], ptr(dk), vp, 4, n, 0, None)
+    assert rc == 0, N.last_error()
+    assert N.lib.trtc_raw_sync(None) == 0
+    p = O.sort_perm(k, False)
+    assert host(dk, NP_OF[name]).tobytes() == k[p].tobytes()
+    gv = host(vbuf, np.uint32)
+    assert gv[off:].tobytes() == v[p].tobytes(), (name, off)
+    assert not gv[:off].any()  # the words before the view are untouched
+
+
 def test_sort_float_nan_rotation(N):
     # NaN in a left slot of the Min_Element tree: the reference output is a rotation
     rng = np.random.default_rng(5)

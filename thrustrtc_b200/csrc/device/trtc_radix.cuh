@@ -314,6 +314,42 @@ TRTC_FORCEINLINE void cp_async_elem(V* smem_dst, const V* gsrc) {
 }
 TRTC_FORCEINLINE void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Bulk copy global -> shared by the tensor memory accelerator (cp.async.bulk, no
+// multicast), completing on a shared-memory mbarrier.  Both addresses 16-byte aligned, the
+// size a multiple of 16.  The copy's shared-memory writes do not use the SM's load/store
+// pipe.
+TRTC_FORCEINLINE uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+TRTC_FORCEINLINE void mbar_init_one(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+    // make the initialised barrier visible to the copy engine (async proxy)
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+TRTC_FORCEINLINE void bulk_load_g2s(void* sdst, const void* gsrc, uint32_t bytes, unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(sdst)),
+                 "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+TRTC_FORCEINLINE bool mbar_try_wait(unsigned long long* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for phase `parity` of the barrier; false when the poll budget is spent
+TRTC_FORCEINLINE bool mbar_wait_bounded(unsigned long long* bar, uint32_t parity, const uint32_t* err) {
+    uint32_t spins = 0;
+    while (!mbar_try_wait(bar, parity))
+        if (!spin_continue(spins, err)) return false;
+    return true;
+}
+
 // Digit of byte `pass` of the ordered key code: one byte permute on the 32-bit half that
 // holds it (sel = 0x4440 | byte index within the half).
 template <class K, bool DESC>
@@ -358,6 +394,14 @@ template <bool B> struct BoolC { static constexpr bool value = B; };
 #ifndef TRTC_RADIX_VASYNC
 #define TRTC_RADIX_VASYNC 1
 #endif
+// 4-byte payloads of a full tile: one bulk copy (cp.async.bulk) of the tile's payloads into
+// the payload staging area, issued when the tile starts and overlapped with the ranking;
+// at staging every thread reads its payloads from there (consecutive words) and, after a
+// barrier, writes them to their staging slots.  Replaces the per-element cp.async copies
+// and their scattered shared-memory writes through the load/store pipe.
+#ifndef TRTC_RADIX_VBULK
+#define TRTC_RADIX_VBULK 1
+#endif
 // the digit masks: two alternating sets of 256 words per warp, placed in the key/payload
 // staging area (idle during the ranking) when it is large enough, else after the counters
 template <int BLOCK>
@@ -368,6 +412,14 @@ constexpr size_t radix_match_smem() {
             (size_t)TILE * (sizeof(KB) + (HAS_VALS ? sizeof(V) : 0)) < radix_match_words<BLOCK>() * 4)
                ? radix_match_words<BLOCK>() * 4 : (size_t)0;
 }
+// the bulk payload path needs 4-byte payloads, a tile of whole 16-byte chunks, and digit
+// masks that do not overlap the payload area (it is filled during the ranking)
+template <class KB, class V, bool HAS_VALS, int BLOCK, int TILE>
+constexpr bool radix_vbulk() {
+    return TRTC_RADIX_VBULK && HAS_VALS && sizeof(V) == 4 && ((size_t)TILE * sizeof(V)) % 16 == 0 &&
+           (TRTC_RADIX_MIXB >= TRTC_RADIX_MIXP || radix_match_smem<KB, V, HAS_VALS, BLOCK, TILE>() != 0 ||
+            (size_t)TILE * sizeof(KB) >= radix_match_words<BLOCK>() * 4);
+}
 
 // HAS_VALS: move a 4- or 8-byte payload with the keys.  vals_from_index: the payload of the
 // first active pass is the element index (used to sort a permutation for odd value sizes).
@@ -377,7 +429,9 @@ constexpr size_t radix_match_smem() {
 //   1. load the keys; rank every key inside its warp (peers of equal digit from bit
 //      ballots or shared-memory digit masks, one shared-memory atomicAdd per peer group on
 //      the warp's digit counters);
-//   2. (payloads are not held in registers: step 4 copies them with cp.async)
+//   2. (payloads are not held in registers across the ranking: a full tile's 4-byte
+//      payloads arrive by one bulk copy issued at the tile's start, others are copied
+//      with cp.async in step 4)
 //   3. one thread per digit: tile count, publication of the tile aggregate, block-wide
 //      exclusive scan of the counts, warp offsets folded into the warp counters;
 //   4. stage keys (and payloads) in shared memory in digit order; then, one thread per
@@ -409,6 +463,8 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
     __shared__ IX s_adj[256];
     __shared__ uint32_t s_wsum[8];
     __shared__ uint32_t s_tile;
+    __shared__ __align__(8) unsigned long long s_vbar;  // completion of the bulk payload copy
+    constexpr bool VB = radix_vbulk<KB, V, HAS_VALS, BLOCK, TILE>();
 
     const int ord = plan.ordinal[pass];
     ST* st = (ord & 1) ? status1 : status0;
@@ -445,6 +501,12 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
     const KB* __restrict__ wk = src_k + wbase;
     const bool full = tile_base + TILE <= n;
     const uint32_t tile_n = full ? (uint32_t)TILE : (uint32_t)(n - tile_base);
+    // uniform over the CTA: full tile, loaded payloads, 16-byte aligned source
+    const bool vbulk = VB && full && !index_payload && ((reinterpret_cast<uintptr_t>(src_v + tile_base) & 15u) == 0);
+    if (vbulk && threadIdx.x == 0) {
+        mbar_init_one(&s_vbar);
+        bulk_load_g2s(s_vals, src_v + tile_base, (uint32_t)(TILE * sizeof(V)), &s_vbar);
+    }
     // keys of this warp inside the tile (partial tiles only)
     const uint32_t warp_n = full ? 32u * ITEMS
                                  : (tile_n > warp * 32u * ITEMS ? min(tile_n - warp * 32u * ITEMS, 32u * ITEMS) : 0u);
@@ -538,29 +600,50 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
     __syncthreads();
 
     // ---- 4. stage in digit order
+    bool bad = false;
+    if (vbulk) {
+        // keys to their slots (rank[] becomes the slot), then the payloads: read from the
+        // bulk-copied tile in the keys' striped order, a barrier, written to the same slots
 #pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-        if (full || (uint32_t)i * 32u + lane < warp_n) {
-            const uint32_t d = radix_digit_sel<K, DESC>(keys[i], sel, hi);
-            const uint32_t pos = wh[d] + rank[i];
-            s_keys[pos] = keys[i];
-            if constexpr (HAS_VALS) {
-                if constexpr (TRTC_RADIX_VASYNC) {
-                    const uint32_t r = (uint32_t)i * 32u + lane;
-                    if (index_payload) s_vals[pos] = (V)(wbase + r);
-                    else cp_async_elem(&s_vals[pos], src_v + wbase + r);
-                } else {
-                    s_vals[pos] = vals[i];
+        for (int i = 0; i < ITEMS; i++) {
+            rank[i] += wh[radix_digit_sel<K, DESC>(keys[i], sel, hi)];
+            s_keys[rank[i]] = keys[i];
+        }
+        if (!mbar_wait_bounded(&s_vbar, 0u, bufs.err)) {
+            report_error(bufs.err, TRTC_ERR_LOOKBACK_TIMEOUT);
+            bad = true;
+        }
+        V pv[VB ? ITEMS : 1];
+        const V* wraw = s_vals + warp * 32u * ITEMS + lane;
+#pragma unroll
+        for (int i = 0; i < (VB ? ITEMS : 1); i++) pv[i] = wraw[i * 32];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < (VB ? ITEMS : 1); i++) s_vals[rank[i]] = pv[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            if (full || (uint32_t)i * 32u + lane < warp_n) {
+                const uint32_t d = radix_digit_sel<K, DESC>(keys[i], sel, hi);
+                const uint32_t pos = wh[d] + rank[i];
+                s_keys[pos] = keys[i];
+                if constexpr (HAS_VALS) {
+                    if constexpr (TRTC_RADIX_VASYNC) {
+                        const uint32_t r = (uint32_t)i * 32u + lane;
+                        if (index_payload) s_vals[pos] = (V)(wbase + r);
+                        else cp_async_elem(&s_vals[pos], src_v + wbase + r);
+                    } else {
+                        s_vals[pos] = vals[i];
+                    }
                 }
             }
         }
+        if constexpr (HAS_VALS && TRTC_RADIX_VASYNC) cp_async_wait_all();  // before the barrier below
     }
-    if constexpr (HAS_VALS && TRTC_RADIX_VASYNC) cp_async_wait_all();  // before the barrier below
 
     // ---- decoupled look-back for the digit's global offset.  Each round polls LB
     // predecessor tiles at once (independent loads), so the inclusive-prefix frontier
     // advances LB tiles per memory round trip.
-    bool bad = false;
     {
         constexpr int LB = TRTC_RADIX_LB;
         ST excl = 0;
