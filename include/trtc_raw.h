@@ -99,8 +99,9 @@ int trtc_raw_segmented_sort_scan(int key_type, void* keys, void* values, void* s
                                  void* workspace, unsigned long long workspace_bytes, int descending, void* stream);
 /* Size classes of the batched kernel: segments of at most `warp_small` (0 or 32) keys are
  * sorted by one warp with a bitonic network (no digit counters), at most 32 x items keys by
- * one warp with 8-bit radix passes, at most 256 x items keys by a whole CTA on chip, longer
- * ones by a whole CTA through global memory; items is 8 or 16.  Per key type, the shape
+ * one warp with 8-bit radix passes, at most 64 / 128 x items keys by a group of two / four
+ * warps, at most 256 x items keys by a whole CTA on chip, longer ones by a whole CTA through
+ * global memory; items is 8 or 16.  Per key type, the shape
  * (items, warp_small) comes from a tuning table: compiled-in defaults (16, 32), a table loaded
  * from the file named by TRTC_SEG_TUNING_FILE at the first batched call, a table passed to
  * trtc_raw_segmented_tuning_load, or the autotuner.

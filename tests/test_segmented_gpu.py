@@ -200,8 +200,9 @@ SHAPES = [(8, 0), (8, 32), (16, 0), (16, 32)]
 @pytest.mark.parametrize("name", ["uint32_t", "float", "int64_t"])
 def test_every_size_class_of_every_shape(N, items, warp_small, name):
     # a table forcing each shape; lengths on both sides of every class limit of that shape:
-    # the bitonic warp class (<= 32), the radix warp class (<= 32 * items), the on-chip CTA
-    # class (<= 256 * items) and the global-memory CTA class
+    # the bitonic warp class (<= 32), the radix warp class (<= 32 * items), the two- and
+    # four-warp groups (<= 64 * items, <= 128 * items), the on-chip CTA class (<= 256 * items)
+    # and the global-memory CTA class
     table = ('{"format": "thrustrtc_b200.segmented_tuning", "version": 1, "entries": '
              '[{"key_type": %d, "items": %d, "warp_small": %d}]}' % (TC[name], items, warp_small))
     old = ctypes.create_string_buffer(4096)
@@ -209,8 +210,10 @@ def test_every_size_class_of_every_shape(N, items, warp_small, name):
     assert N.lib.trtc_raw_segmented_tuning_load(table.encode()) == 0
     try:
         rng = np.random.default_rng(items + warp_small + len(name))
-        lims = [1, 2, 31, 32, 33, 32 * items - 1, 32 * items, 32 * items + 1, 256 * items - 1, 256 * items,
-                256 * items + 1, 3 * 256 * items + 17]
+        lims = [1, 2, 31, 32, 33, 32 * items - 1, 32 * items, 32 * items + 1, 48 * items + 5, 64 * items - 1,
+                64 * items, 64 * items + 1, 100 * items + 3, 128 * items - 1, 128 * items, 128 * items + 1,
+                256 * items - 1, 256 * items, 256 * items + 1, 3 * 256 * items + 17]
+        lims += [64 * items] * 9 + [128 * items - 7] * 5  # several groups of one class at once
         lens = np.array(lims + list(make_lengths(rng, 200, 40, 1.5, 6000)), dtype=np.int64)
         rng.shuffle(lens)
         off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)

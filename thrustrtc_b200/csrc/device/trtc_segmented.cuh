@@ -5,12 +5,15 @@
 // The reference sorts one vector per call (internal/radix_sort.cpp:165-553) and scans one
 // vector per call (internal/general_scan.cpp:8-88); a batch there is one call pair per
 // segment.  Here a CTA takes a segment id from the queue and sorts the whole segment itself,
-// in one of four size classes (the limits are the tuning table's; launch_segmented.cu):
+// in one of six size classes (ITEMS and warp_small are the tuning table's; launch_segmented.cu):
 //   * segments of at most `warp_small` (0 or 32) keys: one warp, a bitonic network over
 //     (code, index) pairs, no digit counters (seg_warp_bitonic);
 //   * segments of at most 32 * ITEMS keys: one warp, four 8-bit LSD passes of ballot
 //     ranking with per-warp counters (seg_warp_sort_scan); a CTA's eight warps take eight
 //     such segments at once;
+//   * segments of at most 64 * ITEMS / 128 * ITEMS keys: a group of two / four warps, the
+//     same passes with the group's counters scanned by the group and named barriers of the
+//     group only (seg_group_sort_scan); a CTA's four / two groups take as many segments;
 //   * small segments (<= 256 * ITEMS keys) are sorted on chip: four 8-bit LSD passes of
 //     warp multisplit ranking + shared-memory scatter, with the tile re-laid out so that
 //     every warp gets keys whatever the segment length; then the values are scanned and
@@ -19,7 +22,8 @@
 //     histograms, then four chunked, stable scatter passes ping-pong between the segment and
 //     a temp array (mostly L2-resident for segments of up to a few MB), then a chunked
 //     scan with a running carry.
-// The queue lists the large segments first, so the longest work starts first.
+// The queue lists the segments by class, largest first, so the longest work starts first and
+// a CTA's batch of small segments shares one class.
 #pragma once
 #include "trtc_prelude.cuh"
 #include "trtc_radix.cuh"
@@ -37,22 +41,55 @@ struct SegItem {
     unsigned long long toff;
 };
 
+// size classes of a segment of `len` keys (items = keys per thread of a CTA tile): 0 one
+// warp, 1 / 2 two / four warps, 3 the CTA on chip, 4 + k the CTA through global memory with
+// floor(log2 len) = floor(log2 (256 items)) + k.  The work queue lists the classes from the
+// largest down, so the longest segments start first.
+enum { SEG_CLASSES = 32 };
+TRTC_FORCEINLINE uint32_t seg_class(unsigned long long len, uint32_t items) {
+    const unsigned long long tile = 256ull * items;
+    if (len > tile) {
+        const int k = (63 - __clzll((long long)len)) - (63 - __clzll((long long)tile));
+        return 4u + (uint32_t)min(k, SEG_CLASSES - 5);
+    }
+    return len > 128ull * items ? 3u : len > 64ull * items ? 2u : len > 32ull * items ? 1u : 0u;
+}
+
 struct SegCtrl {
-    unsigned long long next;        // work-queue cursor
-    unsigned long long front;       // large segments placed from the front
-    unsigned long long back;        // small segments placed from the back
+    unsigned long long next;                   // work-queue cursor
+    unsigned long long count[SEG_CLASSES];     // segments per class
+    unsigned long long placed[SEG_CLASSES];    // segments of a class placed so far
     unsigned long long pad;
 };
 
-// queue[] = large segments (len > tile) first, then small ones
+// per-class segment counts (block histogram, one atomic per class and block)
 template <class OFF>
-__global__ void seg_queue_kernel(const OFF* __restrict__ off, unsigned long long nseg, unsigned long long tile,
-                                 uint32_t* __restrict__ queue, SegCtrl* ctrl) {
+__global__ void __launch_bounds__(256) seg_class_count_kernel(const OFF* __restrict__ off, unsigned long long nseg,
+                                                              uint32_t items, SegCtrl* ctrl) {
+    __shared__ unsigned long long s_c[SEG_CLASSES];
+    if (threadIdx.x < SEG_CLASSES) s_c[threadIdx.x] = 0;
+    __syncthreads();
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < nseg;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        atomicAdd(&s_c[seg_class((unsigned long long)(off[i + 1] - off[i]), items)], 1ull);
+    __syncthreads();
+    if (threadIdx.x < SEG_CLASSES && s_c[threadIdx.x]) atomicAdd(&ctrl->count[threadIdx.x], s_c[threadIdx.x]);
+}
+
+// queue[] = the segments ordered by class, largest class first (order inside a class is free)
+template <class OFF>
+__global__ void __launch_bounds__(256) seg_queue_kernel(const OFF* __restrict__ off, unsigned long long nseg,
+                                                        uint32_t items, uint32_t* __restrict__ queue, SegCtrl* ctrl) {
+    __shared__ unsigned long long s_start[SEG_CLASSES];
+    if (threadIdx.x == 0) {
+        unsigned long long run = 0;
+        for (int c = SEG_CLASSES - 1; c >= 0; c--) { s_start[c] = run; run += ctrl->count[c]; }
+    }
+    __syncthreads();
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < nseg;
          i += (unsigned long long)gridDim.x * blockDim.x) {
-        const unsigned long long len = (unsigned long long)(off[i + 1] - off[i]);
-        if (len > tile) queue[atomicAdd(&ctrl->front, 1ull)] = (uint32_t)i;
-        else queue[nseg - 1 - atomicAdd(&ctrl->back, 1ull)] = (uint32_t)i;
+        const uint32_t c = seg_class((unsigned long long)(off[i + 1] - off[i]), items);
+        queue[s_start[c] + atomicAdd(&ctrl->placed[c], 1ull)] = (uint32_t)i;
     }
 }
 
@@ -248,6 +285,152 @@ __device__ inline void seg_warp_sort_scan(typename RadixKey<K>::B* gk, V* gv, V*
     }
 }
 
+// A group of G (2 or 4) warps sorts (stable LSD, 8-bit digits) and scans a segment of
+// len <= 32 * G * ITEMS keys: the segment is cut into G consecutive warp chunks of 32 * IT
+// elements (element e = wg*32*IT + i*32 + lane in item i of lane `lane` of the group's warp
+// wg, IT = ceil(len / (32 G))); each warp ranks its chunk with ballots and its own 256 digit
+// counters, the group scans the counters digit-major / warp-minor (so equal digits keep the
+// chunk order), and the keys are scattered to the group's staging slice sk.  The values are
+// not held in registers: they move between the group's two value slices va / vb (element e
+// read from the current one, written to its new slot in the other).  Only the group's warps
+// meet at its named barrier `bar` (1 + group index, 32 * G threads), so the CTA's 8 / G
+// groups work on 8 / G segments at once.  s_wsum / s_vpart: one slot per warp of the CTA.
+template <class K, class V, bool DESC, int ITEMS>
+__device__ inline void seg_group_sort_scan(typename RadixKey<K>::B* gk, V* gv, V* gs, uint32_t len,
+                                           typename RadixKey<K>::B* sk, V* va, V* vb, uint32_t* s_whist,
+                                           uint32_t* s_wsum, V* s_vpart, uint32_t G, uint32_t bar) {
+    // G is a runtime value (2 or 4): one copy of this code serves both group sizes, which
+    // keeps the kernel inside its register budget
+    typedef typename RadixKey<K>::B KB;
+    constexpr int D = RadixKey<K>::DIGITS;
+    const uint32_t GT = 32u * G;      // threads of the group
+    const uint32_t DPT = 256u / GT;   // digits scanned per thread
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t wg = warp % G, gw0 = warp - wg;  // warp inside the group, the group's first warp
+    const uint32_t gt = wg * 32u + lane;             // thread inside the group
+    const uint32_t IT = (len + GT - 1u) / GT;        // items in use (group-uniform)
+    const uint32_t wbase = wg * 32u * IT;
+    const uint32_t wn = len > wbase ? min(len - wbase, 32u * IT) : 0u;  // elements of this warp
+    uint32_t* wh = s_whist + warp * 256;
+    const uint32_t ltm = lanemask_lt();
+    // named barrier of the group (immediate ids, so the kernel reserves barriers 0-4 only)
+    auto gsync = [&]() {
+        switch (bar) {
+            case 1: asm volatile("bar.sync 1, %0;\n" ::"r"(GT) : "memory"); break;
+            case 2: asm volatile("bar.sync 2, %0;\n" ::"r"(GT) : "memory"); break;
+            case 3: asm volatile("bar.sync 3, %0;\n" ::"r"(GT) : "memory"); break;
+            default: asm volatile("bar.sync 4, %0;\n" ::"r"(GT) : "memory"); break;
+        }
+    };
+    KB k[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const uint32_t r = (uint32_t)i * 32u + lane;
+        if ((uint32_t)i < IT && r < wn) { k[i] = gk[wbase + r]; va[wbase + r] = gv[wbase + r]; }
+        else k[i] = KB(0);
+    }
+    for (int p = 0; p < D; p++) {
+        const uint32_t sel = 0x4440u | (uint32_t)(p & 3);
+        const bool hi = p >= 4;
+#pragma unroll
+        for (int j = 0; j < 8; j++) wh[j * 32 + lane] = 0;
+        __syncwarp();
+        uint32_t pos[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            pos[i] = 0;
+            if ((uint32_t)i >= IT || (uint32_t)i * 32u >= wn) continue;  // warp-uniform
+            const bool valid = (uint32_t)i * 32u + lane < wn;
+            const uint32_t d = radix_digit_sel<K, DESC>(k[i], sel, hi);
+            uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                const bool set = (d >> b) & 1u;
+                const uint32_t bb = __ballot_sync(0xffffffffu, set);
+                peers &= set ? bb : ~bb;
+            }
+            const uint32_t leader = 31u - __clz(peers | 1u);
+            uint32_t base = 0;
+            if (valid && lane == leader) base = atomicAdd(&wh[d], (uint32_t)__popc(peers));
+            pos[i] = __shfl_sync(0xffffffffu, base, (int)leader) + (uint32_t)__popc(peers & ltm);
+        }
+        gsync();  // every warp's counters are complete
+        // exclusive scan over (digit, warp): thread gt owns digits gt*DPT .. gt*DPT+DPT-1 (the
+        // counts are read again below rather than held in registers)
+        uint32_t tot = 0;
+        for (uint32_t j = 0; j < DPT; j++)
+            for (uint32_t w = 0; w < G; w++) tot += s_whist[(gw0 + w) * 256 + gt * DPT + j];
+        uint32_t inc = tot;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= (uint32_t)d) inc += y;
+        }
+        if (lane == 31) s_wsum[warp] = inc;
+        gsync();
+        uint32_t run = inc - tot;
+        for (uint32_t w = 0; w < wg; w++) run += s_wsum[gw0 + w];
+        for (uint32_t j = 0; j < DPT; j++)
+            for (uint32_t w = 0; w < G; w++) {
+                uint32_t* cw = &s_whist[(gw0 + w) * 256 + gt * DPT + j];
+                const uint32_t c = *cw;
+                *cw = run;
+                run += c;
+            }
+        gsync();  // digit starts of every warp are in place
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t r = (uint32_t)i * 32u + lane;
+            if ((uint32_t)i >= IT || r >= wn) continue;
+            const uint32_t q = pos[i] + wh[radix_digit_sel<K, DESC>(k[i], sel, hi)];
+            sk[q] = k[i];
+            vb[q] = va[wbase + r];
+        }
+        gsync();  // the pass's order is complete in sk / vb
+        if (p + 1 < D) {
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t r = (uint32_t)i * 32u + lane;
+                if ((uint32_t)i < IT && r < wn) k[i] = sk[wbase + r];
+            }
+        }
+        V* t = va; va = vb; vb = t;
+        // the next pass writes sk / vb only after its first group barrier, which every warp
+        // reaches after this reload
+    }
+    // exclusive scan of the sorted values (in va; the sorted keys are in sk): warp totals, the
+    // group's offsets, then each warp's rows with a running carry; keys, values and scan
+    // written in element order
+    V wsum = V();
+#pragma unroll 1
+    for (uint32_t r = lane; r < wn; r += 32u) wsum += va[wbase + r];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) wsum += shfl_xor_any(wsum, d);
+    if (lane == 0) s_vpart[warp] = wsum;
+    gsync();
+    V carry = V();
+    for (uint32_t w = 0; w < wg; w++) carry += s_vpart[gw0 + w];
+#pragma unroll 1
+    for (uint32_t r0 = 0; r0 < wn; r0 += 32u) {  // rows of the warp's chunk (warp-uniform)
+        const uint32_t r = r0 + lane;
+        const bool valid = r < wn;
+        const V x = valid ? va[wbase + r] : V();
+        V incl = x;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const V y = shfl_up_any(incl, d);
+            if (lane >= (uint32_t)d) incl += y;
+        }
+        if (valid) {
+            gk[wbase + r] = sk[wbase + r];
+            gv[wbase + r] = x;
+            if (gs) gs[wbase + r] = carry + incl - x;
+        }
+        carry += shfl_any(incl, 31);
+    }
+    gsync();  // s_vpart and the staging slices are free for the group's next segment
+}
+
 // One warp sorts (and scans) a segment of len <= 32 keys without digit counters: a bitonic
 // network over (ordered code, original index) pairs, one per lane.  The index makes every
 // pair distinct, so the network's result is the stable order (equal codes keep their input
@@ -311,6 +494,11 @@ constexpr size_t seg_sort_scan_smem() {
 // spilling)
 #ifndef TRTC_SEG_MINB
 #define TRTC_SEG_MINB(items, key_bytes) ((key_bytes) > 4 ? 2 : ((items) <= 8 ? 4 : 3))
+#endif
+// groups of two and four warps for the segments between one warp's share and a quarter of
+// the CTA tile (0: those segments take the whole-CTA on-chip class)
+#ifndef TRTC_SEG_GROUPS
+#define TRTC_SEG_GROUPS 1
 #endif
 template <class K, class V, class OFF, bool DESC, int ITEMS, int MINB = TRTC_SEG_MINB(ITEMS, sizeof(K))>
 __global__ void __launch_bounds__(256, MINB) seg_sort_scan_kernel(typename RadixKey<K>::B* __restrict__ keys,
@@ -489,16 +677,20 @@ __global__ void __launch_bounds__(256, MINB) seg_sort_scan_kernel(typename Radix
         unsigned long long base;
         fetch(item, gk, gv, gs, len, base);
         if (len == 0) continue;
-        if (len > WSEG) {
+        if (len > (TRTC_SEG_GROUPS ? 4u : 1u) * WSEG) {
             block_segment(gk, gv, gs, len, base);
             continue;
         }
-        // a small segment: the queue has handed out every large one already, so take seven
-        // more entries and let each warp sort one; entries longer than a warp's share are
-        // deferred to the whole CTA afterwards
-        if (threadIdx.x == 0) s_batch = atomicAdd(&ctrl->next, 7ull);
+        // a small segment: the queue lists the classes from the largest down, so the entries
+        // after it are no longer than its class.  The CTA splits into groups of G warps (one
+        // warp up to WSEG keys, two up to 2 WSEG, four up to 4 WSEG), takes one more entry per
+        // further group, and every group sorts one; an entry longer than its group's share
+        // (list mode keeps the caller's order) is deferred to the whole CTA afterwards
+        const uint32_t G = !TRTC_SEG_GROUPS ? 1u : len > 2u * WSEG ? 4u : (len > WSEG ? 2u : 1u);  // CTA-uniform
+        if (threadIdx.x == 0) s_batch = atomicAdd(&ctrl->next, (unsigned long long)(8u / G - 1u));
         __syncthreads();
-        const unsigned long long mine = warp == 0 ? item : s_batch + warp - 1;
+        const uint32_t grp = warp / G;
+        const unsigned long long mine = grp == 0 ? item : s_batch + grp - 1;
         unsigned long long defer = ~0ull;
         if (mine < nseg) {
             KB* wk;
@@ -507,13 +699,16 @@ __global__ void __launch_bounds__(256, MINB) seg_sort_scan_kernel(typename Radix
             uint32_t wl;
             unsigned long long wb;
             fetch(mine, wk, wv, ws, wl, wb);
-            if (wl > WSEG) defer = mine;
-            else if (wl > 0 && wl <= warp_small) seg_warp_bitonic<K, V, DESC>(wk, wv, ws, wl);
-            else if (wl > 0)
+            if (wl > G * WSEG) defer = mine;
+            else if (wl > 0 && G == 1 && wl <= warp_small) seg_warp_bitonic<K, V, DESC>(wk, wv, ws, wl);
+            else if (wl > 0 && G == 1)
                 seg_warp_sort_scan<K, V, DESC, ITEMS>(wk, wv, ws, wl, s_k + warp * WSEG, s_v + warp * WSEG,
                                                       s_whist + warp * 256);
+            else if (wl > 0)
+                seg_group_sort_scan<K, V, DESC, ITEMS>(wk, wv, ws, wl, s_k + grp * G * WSEG, s_v + grp * G * WSEG,
+                                                       s_o + grp * G * WSEG, s_whist, s_wsum, s_part, G, 1u + grp);
         }
-        if (lane == 0) s_defer[warp] = defer;
+        if (lane == 0) s_defer[warp] = (warp % G == 0) ? defer : ~0ull;
         __syncthreads();
         for (int w = 0; w < 8; w++) {
             const unsigned long long d = s_defer[w];

@@ -1,8 +1,9 @@
 // launch_segmented.cu -- batched segmented sort + exclusive scan (one persistent launch over
 // all segments, fed by a device work queue), its workspace sizing, and the tuning table of
-// size classes: per key type, the items per thread (which sets the one-warp and on-chip class
-// limits, 32 x ITEMS and 256 x ITEMS keys) and the limit of the counter-free warp class (0 or
-// 32 keys), picked by an autotuner from timed trial runs on the batch's own segment lengths and
+// size classes: per key type, the items per thread (which sets the class limits: one warp up
+// to 32 x ITEMS keys, groups of two / four warps up to 64 / 128 x ITEMS, the CTA on chip up to
+// 256 x ITEMS, the CTA through global memory beyond) and the limit of the counter-free warp
+// class (0 or 32 keys), picked by an autotuner from timed trial runs on the batch's own segment lengths and
 // kept as versioned JSON (compiled-in defaults until a table is loaded or tuned).  The digit
 // width is 8 bits in every radix class: on-chip ranking spends one ballot per key bit whatever
 // the width, so narrower digits only add scatter passes and wider ones outgrow a warp's
@@ -26,7 +27,7 @@ using namespace trtc;
 namespace {
 
 struct SegShape {
-    int items;       // items per thread: one-warp class <= 32 x items, on-chip class <= 256 x items
+    int items;       // items per thread: one warp <= 32 x items, 2 / 4 warps <= 64 / 128 x items, CTA on chip <= 256 x items
     int warp_small;  // counter-free (bitonic) warp class limit: 0 (off) or 32 keys
     float ms;        // trial time that chose it (0: compiled-in default or loaded)
 };
@@ -82,7 +83,9 @@ bool seg_run_cfg(void* keys, void* vals, void* scan, const unsigned long long* o
     if (qg > (size_t)sms * 4) qg = (size_t)sms * 4;
     if (qg < 1) qg = 1;
     ktimer_mark("", s);
-    seg_queue_kernel<unsigned long long><<<(unsigned)qg, 256, 0, s>>>(off, nseg, 256ull * ITEMS, queue, ctrl);
+    seg_class_count_kernel<unsigned long long><<<(unsigned)qg, 256, 0, s>>>(off, nseg, (uint32_t)ITEMS, ctrl);
+    seg_queue_kernel<unsigned long long><<<(unsigned)qg, 256, 0, s>>>(off, nseg, (uint32_t)ITEMS, queue, ctrl);
+    count_launch(2);
     ktimer_mark("seg_queue_kernel", s);
     constexpr size_t smem = seg_sort_scan_smem<K, V, ITEMS>();
     auto kernel = seg_sort_scan_kernel<K, V, unsigned long long, DESC, ITEMS>;
@@ -98,7 +101,7 @@ bool seg_run_cfg(void* keys, void* vals, void* scan, const unsigned long long* o
     kernel<<<(unsigned)grid, 256, smem, s>>>((KB*)keys, (V*)vals, (V*)scan, tk, tv, off, queue, nseg, ctrl, nullptr,
                                              warp_small);
     ktimer_mark("seg_sort_scan_kernel", s);
-    count_launch(2);
+    count_launch();
     if constexpr (is_float_key<K>()) {
         seg_rotate_kernel<K, V, unsigned long long, DESC><<<rgrid, 256, 0, s>>>((KB*)keys, (V*)vals, (V*)scan, tk, tv,
                                                                              off, nullptr, nseg, rot);
@@ -143,6 +146,7 @@ std::string tuning_json_locked() {
     std::string j = "{\"format\": \"thrustrtc_b200.segmented_tuning\", \"version\": " +
                     std::to_string(SEG_TUNING_VERSION) +
                     ", \"classes\": [\"warp_bitonic: len <= warp_small\", \"warp_radix: len <= 32*items\", "
+                    "\"group2_radix: len <= 64*items\", \"group4_radix: len <= 128*items\", "
                     "\"cta_onchip: len <= 256*items\", \"cta_global\"], \"digit_bits\": 8, \"entries\": [";
     bool first = true;
     for (const auto& kv : g_seg_tuning) {
