@@ -744,8 +744,26 @@ def run_segmented(args):
     trtc.init()
     L = N.lib
     _seg_sigs(L)
-    nseg = args.n or WORKLOADS["segmented_c4"][0]
-    keys_h, vals_h, off_h = gen_segmented(nseg)
+    if args.seg_len:
+        # one segment length for the whole batch (cost per pair of one size class)
+        nseg = args.n or max(1, (1 << 25) // args.seg_len)
+        n = nseg * args.seg_len
+        off_h = np.arange(0, n + 1, args.seg_len, dtype=np.int64)
+        keys_h = (splitmix64(0, 0, n) >> np.uint64(32)).astype(np.uint32)
+        vals_h = np.arange(n, dtype=np.uint32)
+        lengths = "all %d keys" % args.seg_len
+    else:
+        nseg = args.n or WORKLOADS["segmented_c4"][0]
+        keys_h, vals_h, off_h = gen_segmented(nseg)
+        lengths = "lognormal median 256 sigma 1.5 clipped [1, 2^20]"
+        if args.seg_max:
+            # the same lengths clipped at seg_max (what the longest segments cost); the keys
+            # keep their positions, so the batch is a prefix-preserving cut of each segment
+            lens = np.minimum(np.diff(off_h), args.seg_max)
+            keep = np.concatenate([np.arange(a, a + m) for a, m in zip(off_h[:-1], lens)])
+            keys_h, vals_h = keys_h[keep], np.arange(len(keep), dtype=np.uint32)
+            off_h = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+            lengths += ", then clipped at %d" % args.seg_max
     n = len(keys_h)
     k0 = torch.from_numpy(keys_h.view(np.int32)).to(dev)
     v0 = torch.from_numpy(vals_h.view(np.int32)).to(dev)
@@ -754,9 +772,19 @@ def run_segmented(args):
     wsb = L.trtc_raw_segmented_workspace_bytes(5, n, nseg)
     ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
     P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
-    items = L.trtc_raw_segmented_autotune(5, P(off), nseg, n, None)
-    if items < 0:
-        raise RuntimeError(N.last_error())
+    if args.seg_items:
+        # the shape forced through a tuning table instead of the autotuner
+        L.trtc_raw_segmented_tuning_load.restype = ctypes.c_int
+        L.trtc_raw_segmented_tuning_load.argtypes = [ctypes.c_char_p]
+        table = json.dumps({"format": "thrustrtc_b200.segmented_tuning", "version": 1,
+                            "entries": [{"key_type": 5, "items": args.seg_items, "warp_small": 32}]})
+        if L.trtc_raw_segmented_tuning_load(table.encode()) != 0:
+            raise RuntimeError(N.last_error())
+        items = args.seg_items
+    else:
+        items = L.trtc_raw_segmented_autotune(5, P(off), nseg, n, None)
+        if items < 0:
+            raise RuntimeError(N.last_error())
     stream = torch.cuda.Stream(device=dev)
 
     def call():
@@ -907,11 +935,12 @@ def run_segmented(args):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
                 "data": "synthetic (SplitMix64 seed 0, generated on the host)",
                 "config": {"workload": "segmented_c4", "segments": nseg, "n": n,
-                           "lengths": "lognormal median 256 sigma 1.5 clipped [1, 2^20]",
+                           "lengths": lengths,
                            "keys": "uint32 uniform", "values": "uint32 = index",
                            "op": "stable sort by key per segment, then exclusive Plus scan of its values",
-                           "launch": "1 persistent launch from a device work queue (+1 queue kernel), CUDA graph replay",
-                           "autotuned_items_per_thread": items, "tuning_table": _seg_tuning(L),
+                           "launch": "1 persistent launch from a device work queue (+2 queue kernels), CUDA graph replay",
+                           ("forced_items_per_thread" if args.seg_items else "autotuned_items_per_thread"): items,
+                           "tuning_table": _seg_tuning(L),
                            "parallelism": "replicas x%d" % world,
                            "l2": "inputs (%d MiB) exceed the 126 MB L2" % (8 * n >> 20)},
                 "roofline": {"bound": "hbm", "kernel": "seg_sort_scan_kernel", "achieved": achieved, "peak": peak,
@@ -919,7 +948,7 @@ def run_segmented(args):
                              "frac": (achieved / peak) if achieved else None, "traffic": None,
                              "algorithmic_bytes_per_unit": 20, "launch_ms": per_launch_ms},
                 "plain_per_segment": plain, "cpu_baseline": cpu, "e2e": e2e, "clocks": sampler.summary(),
-                "gpu_launches": 2 * args.steps, "step_ms": [round(x, 4) for x in step_ms]}
+                "gpu_launches": 3 * args.steps, "step_ms": [round(x, 4) for x in step_ms]}
         print(json.dumps(line), flush=True)
     del g
     if world > 1:
@@ -1347,6 +1376,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--allow-short-warmup", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="segmented_c4: skip the per-segment plain calls")
+    ap.add_argument("--seg-len", type=int, default=0, help="segmented_c4: every segment this long (one size class)")
+    ap.add_argument("--seg-max", type=int, default=0, help="segmented_c4: clip the lognormal lengths at this many keys")
+    ap.add_argument("--seg-items", type=int, default=0, choices=[0, 8, 16],
+                    help="segmented_c4: force this items-per-thread shape instead of autotuning")
     ap.add_argument("--no-sub", action="store_true", help="default run: skip the scan / reduce / serving records")
     ap.add_argument("--sub-requests", type=int, default=1000, help="requests of the serving record")
     ap.add_argument("--levels", default="", help="serving_c5: comma-separated fractions of the plain capacity")
