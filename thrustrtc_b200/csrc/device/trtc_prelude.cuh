@@ -96,7 +96,7 @@ TRTC_FORCEINLINE uint32_t lanemask_lt() {
 #ifndef TRTC_SPIN_LIMIT
 #define TRTC_SPIN_LIMIT (1u << 22)
 #endif
-enum : uint32_t { TRTC_ERR_LOOKBACK_TIMEOUT = 1u, TRTC_ERR_BAD_PLAN = 2u };
+enum : uint32_t { TRTC_ERR_LOOKBACK_TIMEOUT = 1u, TRTC_ERR_BAD_PLAN = 2u, TRTC_ERR_BULK_COPY_TIMEOUT = 4u };
 
 TRTC_FORCEINLINE void report_error(uint32_t* err, uint32_t code) {
     if (err) atomicOr(err, code);

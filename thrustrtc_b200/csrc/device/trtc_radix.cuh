@@ -17,7 +17,8 @@
 //     ranks its keys with warp multisplit (bit ballots), publishes per-digit counts,
 //     looks back across earlier tiles for its global offsets (decoupled look-back with
 //     release/acquire flags and bounded spins), stages the tile in shared memory in digit
-//     order and writes it out in bucket runs.
+//     order (a full tile's 4-byte payloads arrive there by one TMA bulk copy issued when the
+//     tile starts) and writes it out in bucket runs.
 #pragma once
 #include "trtc_prelude.cuh"
 
@@ -610,7 +611,7 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
             s_keys[rank[i]] = keys[i];
         }
         if (!mbar_wait_bounded(&s_vbar, 0u, bufs.err)) {
-            report_error(bufs.err, TRTC_ERR_LOOKBACK_TIMEOUT);
+            report_error(bufs.err, TRTC_ERR_BULK_COPY_TIMEOUT);
             bad = true;
         }
         V pv[VB ? ITEMS : 1];

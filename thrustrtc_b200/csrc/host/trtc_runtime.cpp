@@ -166,9 +166,11 @@ bool check_device_errors(cudaStream_t s, const char* what) {
     if (g_err_host && *(volatile uint32_t*)g_err_host) {
         const uint32_t e = *(volatile uint32_t*)g_err_host;
         *(volatile uint32_t*)g_err_host = 0;
-        char buf[160];
-        snprintf(buf, sizeof(buf), "%s: device reported error 0x%x (%s)", what, e,
-                 (e & 1u) ? "look-back wait exceeded its bound" : "inconsistent sort plan");
+        char buf[200];
+        snprintf(buf, sizeof(buf), "%s: device reported error 0x%x (%s%s%s)", what, e,
+                 (e & 1u) ? "look-back wait exceeded its bound; " : "",
+                 (e & 4u) ? "bulk tile copy did not complete within its bound; " : "",
+                 (e & 2u) ? "inconsistent sort plan" : "");
         set_error(buf);
         return false;
     }
