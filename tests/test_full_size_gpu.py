@@ -71,6 +71,20 @@ def test_sort_by_key_u32_pairs_2e28(N, desc):
     check_sorted_pairs(k0, k, v, True, desc)
 
 
+def test_sort_by_key_u32_pairs_past_2e30(N):
+    # n >= 2^30: the digit passes switch to 64-bit look-back status words and positions; the
+    # last tile is partial (its payloads take the per-element copies, the others the bulk copy)
+    import torch
+    n = (1 << 30) + 4099
+    k0 = rand_u32_as_i32(n, 30)
+    k, v = k0.clone(), torch.arange(n, dtype=torch.int32, device="cuda")
+    assert N.lib.trtc_raw_sort_by_key(5, P(k), P(v), 4, n, 0, None) == 0, N.last_error()
+    assert N.lib.trtc_raw_sync(None) == 0, N.last_error()
+    check_sorted_pairs(k0, k, v, True)
+    del k0, k, v
+    torch.cuda.empty_cache()
+
+
 def test_sort_u32_keys_narrow_range_2e28(N):
     # 1000 distinct keys: two of the four digit passes are skipped, the others carry long runs
     import torch
