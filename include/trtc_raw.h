@@ -32,6 +32,11 @@ int trtc_timing_get(int i, char* name, unsigned long long name_cap, float* ms);
  * out-of-memory one does (the call returns its failure value, before any kernel runs, and
  * leaves its inputs untouched); for capacity planning and for tests of those failure paths. */
 void trtc_set_alloc_limit(unsigned long long bytes);
+/* counters of the NVRTC kernel cache since the process started: out[0] NVRTC compilations,
+ * out[1] kernels taken from the persistent cubin cache (TRTC_CACHE_DIR, else
+ * ~/.cache/thrustrtc_b200; TRTC_JIT_DISK_CACHE=0 turns it off), out[2] kernels found already
+ * loaded in this process.  No reference counterpart (its cache has no counters). */
+void trtc_jit_cache_stats(unsigned long long* out);
 /* synchronises `stream`; 0, or -1 when a kernel reported an error */
 int trtc_raw_sync(void* stream);
 

@@ -2,6 +2,7 @@
 // buffers the caller owns, on a caller-chosen stream.  The object-model ABI of
 // include/thrustrtc_b200.h is layered on the same launchers.
 #include <cstring>
+#include "trtc_jit.h"
 #include "trtc_launch.h"
 #include "trtc_runtime.h"
 
@@ -41,6 +42,10 @@ unsigned long long trtc_debug_sort_ctrl(void* host, unsigned long long bytes, vo
 }
 
 void trtc_set_alloc_limit(unsigned long long bytes) { set_alloc_limit(bytes); }
+
+void trtc_jit_cache_stats(unsigned long long* out) {
+    if (out) jit_cache_stats(out);
+}
 
 int trtc_raw_sync(void* stream) {
     if (!ensure_device()) return -1;

@@ -6,7 +6,9 @@
 #include <dlfcn.h>
 #include <nvrtc.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -151,6 +153,7 @@ typedef nvrtcResult (*PFN_nvrtcDestroyProgram)(nvrtcProgram*);
 typedef nvrtcResult (*PFN_nvrtcAddNameExpression)(nvrtcProgram, const char*);
 typedef nvrtcResult (*PFN_nvrtcGetLoweredName)(nvrtcProgram, const char*, const char**);
 typedef const char* (*PFN_nvrtcGetErrorString)(nvrtcResult);
+typedef nvrtcResult (*PFN_nvrtcVersion)(int*, int*);
 
 static struct Nvrtc {
     bool tried = false, ok = false;
@@ -164,6 +167,7 @@ static struct Nvrtc {
     PFN_nvrtcAddNameExpression add_name;
     PFN_nvrtcGetLoweredName lowered;
     PFN_nvrtcGetErrorString err_str;
+    PFN_nvrtcVersion version;  // optional
 } g_nv;
 
 static bool load_nvrtc() {
@@ -191,6 +195,7 @@ static bool load_nvrtc() {
     TRTC_SYM(add_name, "nvrtcAddNameExpression");
     TRTC_SYM(lowered, "nvrtcGetLoweredName");
     TRTC_SYM(err_str, "nvrtcGetErrorString");
+    TRTC_SYM(version, "nvrtcVersion");
 #undef TRTC_SYM
     g_nv.ok = g_nv.create && g_nv.compile && g_nv.cubin && g_nv.add_name && g_nv.lowered;
     if (!g_nv.ok) set_error("NVRTC library lacks required entry points");
@@ -270,6 +275,19 @@ static std::string compose_source(const std::vector<std::string>& headers, const
     return src;
 }
 
+// ------------------------------------------------------------------ persistent cubin cache
+// Compiled cubins persist across processes under cache_dir() (TRTC_CACHE_DIR, else
+// ~/.cache/thrustrtc_b200), so a kernel string costs its NVRTC compilation once per machine,
+// not once per process (the reference keeps such a cache in an unqlite file,
+// internal/impl_context.inl:404-648).  An entry is three files named by a 128-bit hash of its
+// key: <id>.cubin, <id>.name (the kernel's lowered name) and <id>.key, the key itself.  The
+// key holds everything the cubin depends on -- the cache format, a digest of the device
+// headers embedded in this library and of the headers the caller added, NVRTC's version, the
+// architecture, the kernel's name expression and the full source -- and an entry is used only
+// when its stored key equals the key exactly, so neither a hash collision nor an entry written
+// by another build of the library is ever loaded.  The key file is written last, each file by
+// a rename, so a reader sees a complete entry or none.  TRTC_JIT_DISK_CACHE=0 turns the cache
+// off; so do include directories (jit_add_include_dir), whose files the key does not track.
 static std::string cache_dir() {
     const char* e = getenv("TRTC_CACHE_DIR");
     std::string d;
@@ -279,6 +297,84 @@ static std::string cache_dir() {
         d = std::string(home ? home : "/tmp") + "/.cache/thrustrtc_b200";
     }
     return d;
+}
+
+static std::atomic<unsigned long long> g_cache_compiles{0}, g_cache_disk_hits{0}, g_cache_mem_hits{0};
+
+void jit_cache_stats(unsigned long long out[3]) {
+    out[0] = g_cache_compiles.load();
+    out[1] = g_cache_disk_hits.load();
+    out[2] = g_cache_mem_hits.load();
+}
+
+static bool disk_cache_on() {
+    const char* e = getenv("TRTC_JIT_DISK_CACHE");
+    if (e && e[0] == '0' && e[1] == 0) return false;
+    return g_include_dirs.empty();
+}
+
+static std::string hex64(unsigned long long v) {
+    char b[20];
+    snprintf(b, sizeof(b), "%016llx", v);
+    return b;
+}
+
+// digest of the device headers embedded in the library (fixed for a build)
+static const std::string& embedded_headers_digest() {
+    static std::string d;
+    if (d.empty()) {
+        unsigned long long h = fnv1a("trtc embedded headers");
+        for (int i = 0; i < g_num_device_headers; i++) {
+            h = fnv1a(g_device_header_names[i], h);
+            h = fnv1a(std::string("\n") + g_device_header_sources[i], h);
+        }
+        d = hex64(h);
+    }
+    return d;
+}
+
+// digest of the headers added by jit_add_built_in_header (they replace or add to the stubs)
+static std::string user_headers_digest() {
+    unsigned long long h = fnv1a("trtc user headers");
+    for (auto& u : g_user_headers) {
+        h = fnv1a(u.first, h);
+        h = fnv1a("\n" + u.second, h);
+    }
+    return hex64(h);
+}
+
+static std::string nvrtc_version_str() {
+    int ma = 0, mi = 0;
+    if (load_nvrtc() && g_nv.version && g_nv.version(&ma, &mi) == NVRTC_SUCCESS)
+        return std::to_string(ma) + "." + std::to_string(mi);
+    return "unknown";
+}
+
+static std::string cache_key(const std::string& src, const std::string& name_expr) {
+    return "thrustrtc_b200 cubin cache 2\ndevice headers " + embedded_headers_digest() + "\nuser headers " +
+           user_headers_digest() + "\nnvrtc " + nvrtc_version_str() + "\n" + arch_option() + "\nname " + name_expr +
+           "\n" + src;
+}
+
+static bool read_file(const std::string& path, std::string& out) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return false;
+    out.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+    return true;
+}
+
+// writes `data` to `path` through a temporary file and a rename
+static bool write_file_atomic(const std::string& path, const std::string& data) {
+    const std::string tmp = path + ".tmp" + std::to_string((unsigned long long)getpid());
+    {
+        std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
+        if (!f) return false;
+        f.write(data.data(), (std::streamsize)data.size());
+        f.close();
+        if (!f) { remove(tmp.c_str()); return false; }
+    }
+    if (rename(tmp.c_str(), path.c_str()) != 0) { remove(tmp.c_str()); return false; }
+    return true;
 }
 
 static void mkdirs(const std::string& p) {
@@ -357,6 +453,40 @@ static bool nvrtc_compile(const std::string& src, const std::vector<std::string>
     return true;
 }
 
+// The cubin of `src` and, when `name_expr` is given, the lowered name of that kernel: from the
+// disk cache when it holds an entry of exactly this key, else compiled by NVRTC and stored.
+// `from_disk` (optional) tells the caller the cubin came from the cache; `read_disk` false skips
+// the lookup (a cached cubin that the driver refused is compiled again and replaced).
+static bool cubin_for(const std::string& src, const std::string& name_expr, std::string& cubin, std::string& lowered,
+                      bool* from_disk = nullptr, bool read_disk = true) {
+    const bool disk = disk_cache_on();
+    if (from_disk) *from_disk = false;
+    std::string key, base;
+    if (disk) {
+        key = cache_key(src, name_expr);
+        base = cache_dir() + "/" + hex64(fnv1a(key)) + hex64(fnv1a(key, 0x84222325cbf29ce4ull));
+        std::string stored;
+        if (read_disk && read_file(base + ".key", stored) && stored == key && read_file(base + ".cubin", cubin) &&
+            !cubin.empty() && (name_expr.empty() || (read_file(base + ".name", lowered) && !lowered.empty()))) {
+            g_cache_disk_hits++;
+            if (from_disk) *from_disk = true;
+            return true;
+        }
+    }
+    std::vector<std::string> names, low;
+    if (!name_expr.empty()) names.push_back("&" + name_expr);
+    if (!nvrtc_compile(src, names, cubin, low)) return false;
+    g_cache_compiles++;
+    lowered = name_expr.empty() ? std::string() : low[0];
+    if (disk) {
+        // a failed store only costs the next process a compilation
+        mkdirs(cache_dir());
+        if (write_file_atomic(base + ".cubin", cubin) && write_file_atomic(base + ".name", lowered))
+            write_file_atomic(base + ".key", key);
+    }
+    return true;
+}
+
 struct CachedModule {
     CUmodule mod = nullptr;
     CUfunction fn = nullptr;
@@ -378,41 +508,24 @@ bool jit_get_kernel(const std::vector<std::string>& headers, const std::string& 
     std::lock_guard<std::recursive_mutex> lk(g_jit_mu);
     if (!load_driver()) return false;
     const std::string src = compose_source(headers, extra);
-    const std::string key = src + "\n//" + name_expr + "|" + c_name + "|" + arch_option();
+    const std::string key = src + "\n//" + name_expr + "|" + c_name + "|" + arch_option() + "|" + user_headers_digest();
     auto it = g_kernels.find(key);
-    if (it != g_kernels.end()) { out.func = it->second.fn; return true; }
-    char hbuf[32];
-    snprintf(hbuf, sizeof(hbuf), "%016llx", fnv1a(key));
-    const std::string dir = cache_dir();
-    const std::string cpath = dir + "/" + hbuf + ".cubin", npath = dir + "/" + hbuf + ".name";
+    if (it != g_kernels.end()) {
+        g_cache_mem_hits++;
+        out.func = it->second.fn;
+        return true;
+    }
     std::string cubin, lname;
-    {
-        std::ifstream fc(cpath, std::ios::binary), fn(npath);
-        if (fc && fn) {
-            cubin.assign(std::istreambuf_iterator<char>(fc), std::istreambuf_iterator<char>());
-            std::getline(fn, lname);
-        }
-    }
-    if (cubin.empty() || lname.empty()) {
-        std::vector<std::string> lowered;
-        std::vector<std::string> names;
-        if (!name_expr.empty()) names.push_back("&" + name_expr);
-        if (!nvrtc_compile(src, names, cubin, lowered)) return false;
-        lname = name_expr.empty() ? c_name : lowered[0];
-        mkdirs(dir);
-        std::ofstream fc(cpath + ".tmp", std::ios::binary), fn(npath + ".tmp");
-        if (fc && fn) {
-            fc.write(cubin.data(), (std::streamsize)cubin.size());
-            fn << lname << "\n";
-            fc.close();
-            fn.close();
-            rename((cpath + ".tmp").c_str(), cpath.c_str());
-            rename((npath + ".tmp").c_str(), npath.c_str());
-        }
-    }
+    bool from_disk = false;
+    if (!cubin_for(src, name_expr, cubin, lname, &from_disk)) return false;
     CachedModule m;
     CUresult cr = g_drv.load(&m.mod, cubin.data());
+    if (cr != CUDA_SUCCESS && from_disk) {
+        if (!cubin_for(src, name_expr, cubin, lname, nullptr, false)) return false;
+        cr = g_drv.load(&m.mod, cubin.data());
+    }
     if (cr != CUDA_SUCCESS) { set_error("cuModuleLoadData failed"); return false; }
+    if (name_expr.empty()) lname = c_name;
     cr = g_drv.get_function(&m.fn, m.mod, lname.c_str());
     if (cr != CUDA_SUCCESS) { set_error("cuModuleGetFunction failed for " + lname); return false; }
     upload_constants(m.mod);
@@ -458,9 +571,8 @@ bool jit_probe_values(const std::vector<std::string>& exprs, std::vector<unsigne
     for (size_t i = 0; i < exprs.size(); i++) extra += (i ? ", " : "") + std::string("(unsigned long long)(") + exprs[i] + ")";
     extra += "};\n";
     const std::string src = compose_source({}, extra);
-    std::string cubin;
-    std::vector<std::string> lowered;
-    if (!nvrtc_compile(src, {}, cubin, lowered)) return false;
+    std::string cubin, unused;
+    if (!cubin_for(src, std::string(), cubin, unused)) return false;
     CUmodule mod;
     if (g_drv.load(&mod, cubin.data()) != CUDA_SUCCESS) return false;
     CUdeviceptr p;

@@ -73,5 +73,7 @@ bool jit_launch(const JitFunction& f, dim_type grid, dim_type block, unsigned sm
 int jit_block_size(const JitFunction& f, unsigned smem);
 // Device-side values of constant expressions (sizeof / alignof / __builtin_offsetof ...).
 bool jit_probe_values(const std::vector<std::string>& exprs, std::vector<unsigned long long>& out);
+// persistent cubin cache counters: NVRTC compilations, disk-cache hits, in-process hits
+void jit_cache_stats(unsigned long long out[3]);
 
 }  // namespace trtc_host
