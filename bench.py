@@ -5,7 +5,8 @@ Default workload: stable Sort_By_Key of 2^28 uint32 keys (uniform over the 32-bi
 SplitMix64 seed 0) with uint32 values = index, ascending -- the reference's headline case.
 Other workloads (--workload): inclusive scan of 2^28 int32 in [-1000, 1000], reduce of 2^28
 float32 in [0, 1); the mixed-type cases c1_sort_by_key_2e20, c3a_sort_f32,
-c3b_sort_by_key_i64_zipf, c3c_copy_if_functor and c3d_scan_by_key_f32; the batched form
+c3b_sort_by_key_i64_zipf, c3c_copy_if_functor and c3d_scan_by_key_f32; the rows after the
+hot path, f1_reduce_by_key_f32 (Reduce_By_Key) and f2_lower_bound_u32 (Lower_Bound_V); the batched form
 segmented_c4 (100,000 lognormal segments sorted and scanned in one launch, beside one plain
 call pair per segment); and serving_c5 (the request server against one plain call per
 request).
@@ -75,6 +76,14 @@ WORKLOADS = {
                             "GB/s Copy_If 2^28 i32 with a user Functor (x & 1) != 0", "GB/s"),
     "c3d_scan_by_key_f32": (1 << 28, "scan_by_key_kernel", 12, 12,
                             "GB/s inclusive Scan_By_Key 2^28 f32 values, geometric runs", "GB/s"),
+    # the rows after the hot path: by-key reduction (k-means step) and vectorised search
+    # (histogram demo); algorithmic bytes: keys + values read, one key + one sum per run
+    # written (runs of mean 32); queries read, results written (the searched vector's reads
+    # are random and not counted)
+    "f1_reduce_by_key_f32": (1 << 28, None, None, 8.25,
+                             "GB/s Reduce_By_Key 2^28 i32 keys (geometric runs) / f32 values", "GB/s"),
+    "f2_lower_bound_u32": (1 << 26, "jit:trtc::search_v_kernel", 8, 8,
+                           "Gqueries/s Lower_Bound_V 2^26 u32 queries into 2^26 sorted u32", "Gqueries/s"),
     # serving form: a Poisson stream of mixed requests (bounded sample of the 200,000)
     "serving_c5": (1000, None, None, None,
                    "requests/s serving mix 60% sort_by_key 25% scan 15% reduce, sizes 2^10..2^24", "requests/s"),
@@ -985,7 +994,11 @@ def gen_mixed(wl, n):
         return (0x0123456700000000 + pi).astype(np.int64), np.arange(n, dtype=np.int32)
     if wl == "c3c_copy_if_functor":
         return (splitmix64(0, 0, n) >> np.uint64(32)).astype(np.uint32).view(np.int32), None
-    if wl == "c3d_scan_by_key_f32":
+    if wl == "f2_lower_bound_u32":
+        # sorted uint32 keys (the searched vector) and uniform uint32 queries, n of each
+        keys = np.sort((splitmix64(0, 40, n) >> np.uint64(32)).astype(np.uint32))
+        return keys.view(np.int32), (splitmix64(0, 41, n) >> np.uint64(32)).astype(np.uint32).view(np.int32)
+    if wl in ("c3d_scan_by_key_f32", "f1_reduce_by_key_f32"):
         u = _uniform01(0, 30, n)
         heads = u < (1.0 / 32.0)                                         # run lengths ~ Geometric(1/32)
         heads[0] = True
@@ -1046,6 +1059,27 @@ def run_mixed(args):
 
         def step():
             out["count"] = trtc.Copy_If(vin, vout, odd)
+    elif wl == "f1_reduce_by_key_f32":
+        kout, vout_t = torch.empty_like(k0), torch.empty_like(v0)
+        ka, va = trtc.DVVectorAdaptor("int32_t", n, k0.data_ptr()), trtc.DVVectorAdaptor("float", n, v0.data_ptr())
+        koa = trtc.DVVectorAdaptor("int32_t", n, kout.data_ptr())
+        voa = trtc.DVVectorAdaptor("float", n, vout_t.data_ptr())
+
+        def restore():
+            flush.fill_(1)
+
+        def step():
+            out["count"] = trtc.Reduce_By_Key(ka, va, koa, voa)
+    elif wl == "f2_lower_bound_u32":
+        res = torch.empty_like(v0)
+        sa, qa = trtc.DVVectorAdaptor("uint32_t", n, k0.data_ptr()), trtc.DVVectorAdaptor("uint32_t", n, v0.data_ptr())
+        ra = trtc.DVVectorAdaptor("int32_t", n, res.data_ptr())
+
+        def restore():
+            flush.fill_(1)
+
+        def step():
+            trtc.Lower_Bound_V(sa, qa, ra)
     else:
         dst = torch.empty_like(v0)
 
@@ -1077,7 +1111,7 @@ def run_mixed(args):
         raise RuntimeError(N.last_error())
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ms = sum(step_ms) / args.steps
-    value = n / (ms / 1e3) / 1e9 if unit == "Gkeys/s" else b_unit * n / (ms / 1e3) / 1e9
+    value = n / (ms / 1e3) / 1e9 if unit in ("Gkeys/s", "Gqueries/s") else b_unit * n / (ms / 1e3) / 1e9
 
     # ---- size-independent checks of the last step
     if wl in ("c1_sort_by_key_2e20", "c3b_sort_by_key_i64_zipf"):
@@ -1097,6 +1131,22 @@ def run_mixed(args):
     elif wl == "c3c_copy_if_functor":
         sel = k0[(k0 & 1) != 0]
         ok = out["count"] == sel.numel() and torch.equal(dst[: sel.numel()], sel)
+    elif wl == "f1_reduce_by_key_f32":
+        # one (key, sum) per run, in order; sums against float64 within 1e-5 (values >= 0)
+        ukeys, counts = torch.unique_consecutive(k0, return_counts=True)
+        m = ukeys.numel()
+        ends = torch.cumsum(counts, 0)
+        cs = torch.cumsum(v0.view(torch.float32).to(torch.float64), 0)
+        ref = cs[ends - 1] - torch.cat([torch.zeros(1, dtype=torch.float64, device=dev), cs[ends[:-1] - 1]])
+        got = vout_t[:m].view(torch.float32).to(torch.float64)
+        rel = ((got - ref).abs() / ref.abs().clamp_min(1e-30)).max().item() if m else 0.0
+        out["runs"] = m
+        out["max_rel_err_vs_fp64"] = rel
+        ok = out["count"] == m and torch.equal(kout[:m], ukeys) and rel <= 1e-5
+    elif wl == "f2_lower_bound_u32":
+        mask = 0xFFFFFFFF
+        exp = torch.searchsorted(k0.to(torch.int64) & mask, v0.to(torch.int64) & mask, right=False)
+        ok = torch.equal(res.to(torch.int64), exp)
     else:
         seg_start = torch.nonzero(torch.cat([torch.ones(1, dtype=torch.bool, device=dev), k0[1:] != k0[:-1]]))[:, 0]
         cs = torch.cumsum(v0.view(torch.float32).to(torch.float64), 0)
@@ -1118,6 +1168,14 @@ def run_mixed(args):
     peak, peak_src = measured_peak()
     per_launch_ms = statistics.mean(kt) if kt else None
     achieved = b_launch * n / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else None
+    if kname is None:
+        # a composed call (Reduce_By_Key: segmented scan + compaction): its algorithmic bytes
+        # over the device time of all its kernels per call
+        kname = "all kernels of the call"
+        kt = [t for _, t in recs]
+        per_launch_ms = sum(kt) / args.steps if kt else None
+        b_launch = b_unit
+        achieved = b_unit * n / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else None
     share = {}
     for name, t in recs:
         share[name] = share.get(name, 0.0) + t
@@ -1125,7 +1183,8 @@ def run_mixed(args):
             "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"c1_sort_by_key_2e20": "u32", "c3a_sort_f32": "f32",
                                            "c3b_sort_by_key_i64_zipf": "int64", "c3c_copy_if_functor": "int32",
-                                           "c3d_scan_by_key_f32": "f32"}[wl],
+                                           "c3d_scan_by_key_f32": "f32", "f1_reduce_by_key_f32": "i32/f32",
+                                           "f2_lower_bound_u32": "u32"}[wl],
             "data": "synthetic (SplitMix64 seed 0, generated on the host)",
             "config": {"workload": wl, "n": n, "l2": "inputs exceed the 126 MB L2 (flush between steps for "
                                                      "non-destructive ops)" if n > (1 << 24) else
@@ -1400,7 +1459,7 @@ def main():
         return run_segmented(args)
     if args.workload == "serving_c5":
         return run_serving(args)
-    if args.workload.startswith(("c1_", "c3")):
+    if args.workload.startswith(("c1_", "c3", "f1_", "f2_")):
         return run_mixed(args)
     return run_ours(args)
 

@@ -24,6 +24,23 @@ enum CompactMode : int {
     CM_TAIL = 7,             // i == n-1 || !pred(in[i], in[i+1]) reduce_by_key segment tails
 };
 
+// Element i of a view through the read-only path (ld.global.nc) when the view is contiguous
+// and its elements are 4 or 8 bytes: the second array of the two-array forms is read at the
+// selected elements only, and a read-only load can be issued ahead of the kernel's stores
+// (which the compiler cannot prove do not alias it) instead of each one waiting behind them.
+template <class T, class V>
+TRTC_FORCEINLINE T ld_view_nc(const V& v, size_t i) {
+    if constexpr (ViewTraits<V>::contiguous && sizeof(T) == 4) {
+        const unsigned int b = __ldg(reinterpret_cast<const unsigned int*>(v._data + i));
+        return *reinterpret_cast<const T*>(&b);
+    } else if constexpr (ViewTraits<V>::contiguous && sizeof(T) == 8) {
+        const unsigned long long b = __ldg(reinterpret_cast<const unsigned long long*>(v._data + i));
+        return *reinterpret_cast<const T*>(&b);
+    } else {
+        return (T)v[i];
+    }
+}
+
 // CT: type of the selected counts (32-bit while n < 2^32: flag and count then travel in one
 // 64-bit look-back word)
 template <int MODE, bool PARTITION, bool TWO, class InV, class StV, class Pred, class ValT, class OutV, class FalseV,
@@ -160,10 +177,16 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
     __shared__ CT s_pre;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     const uint32_t ltm = lanemask_lt();
-    // 16-byte vector path for full, aligned tiles of 4-byte elements under element-wise
-    // selections: lane l of a warp row holds 4 consecutive elements
-    constexpr bool VECOK = ViewTraits<InV>::contiguous && ViewTraits<OutV>::contiguous && sizeof(E) == 4 && !TWO &&
-                           !PARTITION && (MODE == CM_PRED || MODE == CM_NOT_EQUAL || MODE == CM_NOT_PRED);
+    // 16-byte vector path for full, aligned tiles of 4-byte elements: lane l of a warp row
+    // holds 4 consecutive elements.  Element-wise selections, and the neighbour tests of
+    // unique (previous element) and of segment tails (next element), whose neighbours come
+    // from the lane's own vector, the adjacent lane (shuffle), the adjacent row, or one global
+    // load at the edge of the warp's segment; a second array (TWO) is read and written only
+    // at the selected elements
+    constexpr bool NEIGH = MODE == CM_UNIQUE || MODE == CM_UNIQUE_PRED || MODE == CM_TAIL;
+    constexpr bool VECOK = ViewTraits<InV>::contiguous && ViewTraits<OutV>::contiguous && sizeof(E) == 4 && !PARTITION &&
+                           (MODE == CM_PRED || MODE == CM_NOT_EQUAL || MODE == CM_NOT_PRED || NEIGH) &&
+                           (!TWO || NEIGH);
     constexpr int VROWS = ITEMS / 4;
     typedef union { uint4 q; E t[4]; } Vec;
     // vector path: each warp gathers its selected elements in shared memory (placed so that
@@ -179,7 +202,44 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
         if constexpr (MODE == CM_PRED) return (bool)pred(x);
         else if constexpr (MODE == CM_NOT_EQUAL) return !(x == value);
         else if constexpr (MODE == CM_NOT_PRED) return !(bool)pred(x);
-        else return false;  // not used (VECOK excludes the other modes)
+        else return false;  // not used (the neighbour modes take row_flags)
+    };
+    // selections of row r of a warp segment starting at element wbase (rows u[0..VROWS) of
+    // the segment in registers; edge_v: the element before the segment (unique) or after it
+    // (tails), read by the caller where it exists)
+    auto row_flags = [&](const Vec* u, int r, const E& edge_v, size_t wbase, bool (&f)[4]) {
+        if constexpr (!NEIGH) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) f[e] = vsel(u[r].t[e]);
+        } else {
+            const size_t i0 = wbase + (size_t)r * 128 + (size_t)lane * 4;
+            if constexpr (MODE == CM_TAIL) {
+                E nx = shfl_down_any(u[r].t[0], 1);
+                const E nrow = (r + 1 < VROWS) ? shfl_any(u[r + 1 < VROWS ? r + 1 : r].t[0], 0) : edge_v;
+                if (lane == 31) nx = nrow;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const E next = e < 3 ? u[r].t[e < 3 ? e + 1 : 3] : nx;
+                    f[e] = i0 + e + 1 == n || !(bool)pred(u[r].t[e], next);
+                }
+            } else {
+                E pv = shfl_up_any(u[r].t[3], 1);
+                const E prow = r > 0 ? shfl_any(u[r > 0 ? r - 1 : 0].t[3], 31) : edge_v;
+                if (lane == 0) pv = prow;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const E prev = e > 0 ? u[r].t[e > 0 ? e - 1 : 0] : pv;
+                    if constexpr (MODE == CM_UNIQUE) f[e] = i0 + e == 0 || u[r].t[e] != prev;
+                    else f[e] = i0 + e == 0 || !(bool)pred(u[r].t[e], prev);
+                }
+            }
+        }
+    };
+    // the neighbour outside the warp segment [wbase, wbase + 32*ITEMS) (all lanes read it)
+    auto edge_of = [&](size_t wbase) -> E {
+        if constexpr (MODE == CM_TAIL) return wbase + 32 * ITEMS < n ? (E)in._data[wbase + 32 * ITEMS] : E();
+        else if constexpr (NEIGH) return wbase > 0 ? (E)in._data[wbase - 1] : E();
+        else return E();
     };
 
     auto claim = [&]() -> size_t {
@@ -229,14 +289,29 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
         uint32_t wc = 0;
         if (vec_fast(tile)) {
             if constexpr (VECOK) {
-                const uint4* p = reinterpret_cast<const uint4*>(in._data + tile * TILE + (size_t)warp * 32 * ITEMS);
+                const size_t wb = tile * TILE + (size_t)warp * 32 * ITEMS;
+                const uint4* p = reinterpret_cast<const uint4*>(in._data + wb);
                 uint32_t c = 0;
+                if constexpr (NEIGH) {
+                    Vec u[VROWS];
 #pragma unroll
-                for (int r = 0; r < VROWS; r++) {
-                    Vec u;
-                    u.q = p[r * 32 + lane];
+                    for (int r = 0; r < VROWS; r++) u[r].q = p[r * 32 + lane];
+                    const E edge = edge_of(wb);
 #pragma unroll
-                    for (int e = 0; e < 4; e++) c += vsel(u.t[e]) ? 1u : 0u;
+                    for (int r = 0; r < VROWS; r++) {
+                        bool f[4];
+                        row_flags(u, r, edge, wb, f);
+#pragma unroll
+                        for (int e = 0; e < 4; e++) c += f[e] ? 1u : 0u;
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < VROWS; r++) {
+                        Vec u;
+                        u.q = p[r * 32 + lane];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) c += vsel(u.t[e]) ? 1u : 0u;
+                    }
                 }
                 wc = __reduce_add_sync(0xffffffffu, c);
             }
@@ -287,10 +362,12 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
             if constexpr (VECOK) {
                 unsigned long long run = s_pre;
                 for (uint32_t w = 0; w < warp; w++) run += s_wcnt[buf][w];
-                const uint4* p = reinterpret_cast<const uint4*>(in._data + cur * TILE + (size_t)warp * 32 * ITEMS);
+                const size_t wb = cur * TILE + (size_t)warp * 32 * ITEMS;
+                const uint4* p = reinterpret_cast<const uint4*>(in._data + wb);
                 Vec u[VROWS];
 #pragma unroll
                 for (int r = 0; r < VROWS; r++) u[r].q = p[r * 32 + lane];
+                const E edge = edge_of(wb);
                 const unsigned long long out_n = out.size();
                 E* sbuf = s_stage + warp * WSTAGE;
                 // slot j of sbuf holds output element run + (j - s0)
@@ -300,8 +377,9 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
                 for (int r = 0; r < VROWS; r++) {
                     bool f[4];
                     uint32_t c = 0;
+                    row_flags(u, r, edge, wb, f);
 #pragma unroll
-                    for (int e = 0; e < 4; e++) { f[e] = vsel(u[r].t[e]); c += f[e] ? 1u : 0u; }
+                    for (int e = 0; e < 4; e++) c += f[e] ? 1u : 0u;
                     uint32_t x = c;  // inclusive prefix of the lane counts
 #pragma unroll
                     for (int d = 1; d < 32; d <<= 1) {
@@ -310,8 +388,15 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
                     }
                     uint32_t pos = s0 + tot + (x - c);
 #pragma unroll
-                    for (int e = 0; e < 4; e++)
-                        if (f[e]) sbuf[pos++] = u[r].t[e];
+                    for (int e = 0; e < 4; e++) {
+                        if (!f[e]) continue;
+                        if constexpr (TWO) {  // the second array at the selected element, stored singly
+                            const unsigned long long g = run + (pos - s0);
+                            if (g < (unsigned long long)out2.size())
+                                out2[g] = ld_view_nc<E2>(in2, wb + (size_t)r * 128 + (size_t)lane * 4 + e);
+                        }
+                        sbuf[pos++] = u[r].t[e];
+                    }
                     tot += __shfl_sync(0xffffffffu, x, 31);
                 }
                 __syncwarp();
@@ -334,15 +419,10 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
             E v[ITEMS];
             bool f[ITEMS];
             load(cur, v, f);
-            E2 v2[TWO ? ITEMS : 1];
+            // TWO: the second array is read at the selected elements only (the outputs never
+            // overlap the inputs in this kernel); a register copy of the whole row set would
+            // read all of it and spill
             const size_t wbase = cur * TILE + (size_t)warp * 32 * ITEMS;
-            if constexpr (TWO) {
-#pragma unroll
-                for (int i = 0; i < ITEMS; i++) {
-                    const size_t idx = wbase + (size_t)i * 32 + lane;
-                    v2[i] = idx < n ? (E2)in2[idx] : E2();
-                }
-            }
             unsigned long long base = s_pre;
             for (uint32_t w = 0; w < warp; w++) base += s_wcnt[buf][w];
             const size_t out_n = out.size();
@@ -358,7 +438,7 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
                     if (before < out_n) {
                         out[before] = v[i];
                         if constexpr (TWO) {
-                            if (before < (unsigned long long)out2.size()) out2[before] = v2[i];
+                            if (before < (unsigned long long)out2.size()) out2[before] = ld_view_nc<E2>(in2, idx);
                         }
                     }
                 } else {

@@ -251,6 +251,9 @@ bool scan_by_key_raw(int ktc, int vtc, int mode, const void* keys, const void* v
 #ifndef TRTC_COMPACT2_ITEMS
 #define TRTC_COMPACT2_ITEMS 32  // elements per thread of a two-phase compaction tile
 #endif
+#ifndef TRTC_COMPACT2_GENERIC_ITEMS
+#define TRTC_COMPACT2_GENERIC_ITEMS 16  // the same for the forms outside the 16-byte vector path
+#endif
 
 template <class T, int MODE, class CT>
 static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_t s, unsigned long long* count) {
@@ -273,7 +276,10 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
         }
         (void)cudaGetLastError();  // the failed allocation must not fail the launch check below
     }
-    constexpr int ITEMS1 = 16, ITEMS2 = TRTC_COMPACT2_ITEMS;
+    // the vector path (4-byte elements: remove's element-wise test, unique's neighbour test)
+    // takes TRTC_COMPACT2_ITEMS; other widths take TRTC_COMPACT2_GENERIC_ITEMS
+    constexpr bool VEC = sizeof(T) == 4 && (MODE == CM_NOT_EQUAL || MODE == CM_UNIQUE);
+    constexpr int ITEMS1 = 16, ITEMS2 = VEC ? TRTC_COMPACT2_ITEMS : TRTC_COMPACT2_GENERIC_ITEMS;
     const int ITEMS = disjoint ? ITEMS2 : ITEMS1;
     const size_t TILE = (size_t)SCAN_BLOCK * ITEMS;
     const size_t tiles = (n + TILE - 1) / TILE;

@@ -454,6 +454,9 @@ bool TRTC_Copy(const DVVectorLike& vec_in, DVVectorLike& vec_out) {
 }
 
 // ====================================================================== compaction family
+#ifndef TRTC_COMPACT2_GENERIC_ITEMS
+#define TRTC_COMPACT2_GENERIC_ITEMS 16  // 2^28 int32 unique outside the vector path: 16 items 0.69 ms, 32 0.77-0.99
+#endif
 namespace {
 enum { CM_PRED = 0, CM_PRED_STENCIL = 1, CM_NOT_EQUAL = 2, CM_NOT_PRED = 3, CM_NOT_PRED_STENCIL = 4, CM_UNIQUE = 5,
        CM_UNIQUE_PRED = 6, CM_TAIL = 7 };
@@ -540,7 +543,16 @@ unsigned long long run_compact(CompactSpec& c) {
         }
         (void)cudaGetLastError();  // the failed allocation must not fail a later launch check
     }
-    const size_t tile = 256 * (two_phase ? 32 : 16);
+    // the 16-byte vector path (contiguous 4-byte input and output: element-wise tests of one
+    // array, or neighbour tests with an optional second array) takes 32 items per thread; the
+    // other two-phase forms (views, other widths, stencils, partitions) hold their rows in
+    // registers and take TRTC_COMPACT2_GENERIC_ITEMS
+    const bool neigh = c.mode == CM_UNIQUE || c.mode == CM_UNIQUE_PRED || c.mode == CM_TAIL;
+    const bool vec_mode = !c.partition && c.in->elem_size() == 4 && c.in->contiguous_data() && !c.written.empty() &&
+                          c.written[0]->contiguous_data() &&
+                          ((!c.two && (c.mode == CM_PRED || c.mode == CM_NOT_EQUAL || c.mode == CM_NOT_PRED)) || neigh);
+    const int items2 = vec_mode ? 32 : TRTC_COMPACT2_GENERIC_ITEMS;
+    const size_t tile = 256 * (two_phase ? (size_t)items2 : 16);
     const size_t tiles = (n + tile - 1) / tile;
     ViewBuf st;
     trtc::LookbackState lst;
@@ -550,7 +562,7 @@ unsigned long long run_compact(CompactSpec& c) {
                           ", " + (c.partition ? "true" : "false") + ", " + (c.two ? "true" : "false") + ", " +
                           iv.type + ", " + sv.type + ", " + ptype + ", " + vtype + ", " + c.out.type + ", " +
                           c.out_false.type + ", " + c.in2.type + ", " + c.out2.type + ", 256, " +
-                          (two_phase ? "32, " : "16, ") +
+                          (two_phase ? std::to_string(items2) + ", " : std::string("16, ")) +
                           (c32 ? "unsigned int" : "unsigned long long") + ">";
     std::vector<ViewBuf> params{iv.bytes, sv.bytes, pbytes, vbytes, c.out.bytes, c.out_false.bytes, c.in2.bytes,
                                 c.out2.bytes, pod_bytes<size_t>(n)};
