@@ -5,7 +5,7 @@ Default workload: stable Sort_By_Key of 2^28 uint32 keys (uniform over the 32-bi
 SplitMix64 seed 0) with uint32 values = index, ascending -- the reference's headline case.
 Other workloads (--workload): inclusive scan of 2^28 int32 in [-1000, 1000], reduce of 2^28
 float32 in [0, 1); the mixed-type cases c1_sort_by_key_2e20, c3a_sort_f32,
-c3b_sort_by_key_i64_zipf, c3c_copy_if_functor and c3d_scan_by_key_f32; the rows after the
+c3b_sort_by_key_i64_zipf, c3c_copy_if_functor, c3d_scan_by_key_f32 and a13_unique_i32; the rows after the
 hot path, f1_reduce_by_key_f32 (Reduce_By_Key) and f2_lower_bound_u32 (Lower_Bound_V); the batched form
 segmented_c4 (100,000 lognormal segments sorted and scanned in one launch, beside one plain
 call pair per segment); and serving_c5 (the request server against one plain call per
@@ -80,6 +80,8 @@ WORKLOADS = {
     # (histogram demo); algorithmic bytes: keys + values read, one key + one sum per run
     # written (runs of mean 32); queries read, results written (the searched vector's reads
     # are random and not counted)
+    "a13_unique_i32": (1 << 28, "compact_kernel", 4.125, 4.125,
+                       "GB/s Unique (copy) 2^28 i32 in geometric runs of mean 32", "GB/s"),
     "f1_reduce_by_key_f32": (1 << 28, None, None, 8.25,
                              "GB/s Reduce_By_Key 2^28 i32 keys (geometric runs) / f32 values", "GB/s"),
     "f2_lower_bound_u32": (1 << 26, "jit:trtc::search_v_kernel", 8, 8,
@@ -998,6 +1000,9 @@ def gen_mixed(wl, n):
         # sorted uint32 keys (the searched vector) and uniform uint32 queries, n of each
         keys = np.sort((splitmix64(0, 40, n) >> np.uint64(32)).astype(np.uint32))
         return keys.view(np.int32), (splitmix64(0, 41, n) >> np.uint64(32)).astype(np.uint32).view(np.int32)
+    if wl == "a13_unique_i32":
+        k, _ = gen_mixed("c3d_scan_by_key_f32", n)
+        return k, None
     if wl in ("c3d_scan_by_key_f32", "f1_reduce_by_key_f32"):
         u = _uniform01(0, 30, n)
         heads = u < (1.0 / 32.0)                                         # run lengths ~ Geometric(1/32)
@@ -1059,6 +1064,17 @@ def run_mixed(args):
 
         def step():
             out["count"] = trtc.Copy_If(vin, vout, odd)
+    elif wl == "a13_unique_i32":
+        dst = torch.empty_like(k0)
+
+        def restore():
+            flush.fill_(1)
+
+        def step():
+            c = L.trtc_raw_unique_copy(4, P(k0), P(dst), n, None)
+            if c == (1 << 64) - 1:
+                raise RuntimeError(N.last_error())
+            out["count"] = c
     elif wl == "f1_reduce_by_key_f32":
         kout, vout_t = torch.empty_like(k0), torch.empty_like(v0)
         ka, va = trtc.DVVectorAdaptor("int32_t", n, k0.data_ptr()), trtc.DVVectorAdaptor("float", n, v0.data_ptr())
@@ -1131,6 +1147,9 @@ def run_mixed(args):
     elif wl == "c3c_copy_if_functor":
         sel = k0[(k0 & 1) != 0]
         ok = out["count"] == sel.numel() and torch.equal(dst[: sel.numel()], sel)
+    elif wl == "a13_unique_i32":
+        exp = torch.unique_consecutive(k0)
+        ok = out["count"] == exp.numel() and torch.equal(dst[: exp.numel()], exp)
     elif wl == "f1_reduce_by_key_f32":
         # one (key, sum) per run, in order; sums against float64 within 1e-5 (values >= 0)
         ukeys, counts = torch.unique_consecutive(k0, return_counts=True)
@@ -1184,7 +1203,7 @@ def run_mixed(args):
             "vs_baseline": None, "dtype": {"c1_sort_by_key_2e20": "u32", "c3a_sort_f32": "f32",
                                            "c3b_sort_by_key_i64_zipf": "int64", "c3c_copy_if_functor": "int32",
                                            "c3d_scan_by_key_f32": "f32", "f1_reduce_by_key_f32": "i32/f32",
-                                           "f2_lower_bound_u32": "u32"}[wl],
+                                           "f2_lower_bound_u32": "u32", "a13_unique_i32": "int32"}[wl],
             "data": "synthetic (SplitMix64 seed 0, generated on the host)",
             "config": {"workload": wl, "n": n, "l2": "inputs exceed the 126 MB L2 (flush between steps for "
                                                      "non-destructive ops)" if n > (1 << 24) else
@@ -1459,7 +1478,7 @@ def main():
         return run_segmented(args)
     if args.workload == "serving_c5":
         return run_serving(args)
-    if args.workload.startswith(("c1_", "c3", "f1_", "f2_")):
+    if args.workload.startswith(("c1_", "c3", "f1_", "f2_", "a13_")):
         return run_mixed(args)
     return run_ours(args)
 

@@ -41,6 +41,13 @@ TRTC_FORCEINLINE T ld_view_nc(const V& v, size_t i) {
     }
 }
 
+// the element array of a contiguous view (nullptr for the others)
+template <class T, class V>
+TRTC_FORCEINLINE const T* view_ptr(const V& v) {
+    if constexpr (ViewTraits<V>::contiguous) return reinterpret_cast<const T*>(v._data);
+    else return nullptr;
+}
+
 // CT: type of the selected counts (32-bit while n < 2^32: flag and count then travel in one
 // 64-bit look-back word)
 template <int MODE, bool PARTITION, bool TWO, class InV, class StV, class Pred, class ValT, class OutV, class FalseV,
@@ -189,6 +196,8 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
                            (!TWO || NEIGH);
     constexpr int VROWS = ITEMS / 4;
     typedef union { uint4 q; E t[4]; } Vec;
+    // a contiguous second array of 4-byte elements (its rows can be read as 16-byte vectors)
+    constexpr bool VEC2 = ViewTraits<In2V>::contiguous && sizeof(E2) == 4;
     // vector path: each warp gathers its selected elements in shared memory (placed so that
     // 16-byte aligned output addresses map to 16-byte aligned slots), then writes them with
     // 16-byte stores (scalar stores only at the run's ragged ends)
@@ -301,8 +310,13 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
                     for (int r = 0; r < VROWS; r++) {
                         bool f[4];
                         row_flags(u, r, edge, wb, f);
+                        uint32_t rc = 0;
 #pragma unroll
-                        for (int e = 0; e < 4; e++) c += f[e] ? 1u : 0u;
+                        for (int e = 0; e < 4; e++) rc += f[e] ? 1u : 0u;
+                        c += rc;
+                        // the second array's selected rows into L2 for phase 2 (one tile later)
+                        if constexpr (TWO && VEC2)
+                            if (rc) asm volatile("prefetch.global.L2 [%0];" ::"l"(view_ptr<E2>(in2) + wb + (size_t)r * 128 + (size_t)lane * 4));
                     }
                 } else {
 #pragma unroll
@@ -372,12 +386,38 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
                 E* sbuf = s_stage + warp * WSTAGE;
                 // slot j of sbuf holds output element run + (j - s0)
                 const uint32_t s0 = (uint32_t)((reinterpret_cast<size_t>(out._data + run) >> 2) & 3u);
+                // two-array forms with a 16-byte aligned, contiguous 4-byte second array: every
+                // row's selections first, then one 16-byte load per row holding a selected
+                // element, all issued before any store (a load per selected element placed at
+                // its store waits a memory round trip per row)
+                constexpr bool PRE2 = TWO && VEC2;
+                uint32_t fmask = 0;
+                Vec u2[PRE2 ? VROWS : 1];
+                const bool pre2 = PRE2 && ((reinterpret_cast<size_t>(view_ptr<E2>(in2) + wb) & 15u) == 0);
+                if (PRE2 && pre2) {
+#pragma unroll
+                    for (int r = 0; r < VROWS; r++) {
+                        bool f[4];
+                        row_flags(u, r, edge, wb, f);
+#pragma unroll
+                        for (int e = 0; e < 4; e++) fmask |= (f[e] ? 1u : 0u) << (r * 4 + e);
+                    }
+#pragma unroll
+                    for (int r = 0; r < (PRE2 ? VROWS : 1); r++)
+                        if ((fmask >> (r * 4)) & 15u)
+                            u2[r].q = __ldg(reinterpret_cast<const uint4*>(view_ptr<E2>(in2) + wb + (size_t)r * 128) + lane);
+                }
                 uint32_t tot = 0;
 #pragma unroll
                 for (int r = 0; r < VROWS; r++) {
                     bool f[4];
                     uint32_t c = 0;
-                    row_flags(u, r, edge, wb, f);
+                    if (PRE2 && pre2) {
+#pragma unroll
+                        for (int e = 0; e < 4; e++) f[e] = (fmask >> (r * 4 + e)) & 1u;
+                    } else {
+                        row_flags(u, r, edge, wb, f);
+                    }
 #pragma unroll
                     for (int e = 0; e < 4; e++) c += f[e] ? 1u : 0u;
                     uint32_t x = c;  // inclusive prefix of the lane counts
@@ -392,8 +432,10 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
                         if (!f[e]) continue;
                         if constexpr (TWO) {  // the second array at the selected element, stored singly
                             const unsigned long long g = run + (pos - s0);
-                            if (g < (unsigned long long)out2.size())
-                                out2[g] = ld_view_nc<E2>(in2, wb + (size_t)r * 128 + (size_t)lane * 4 + e);
+                            if (g < (unsigned long long)out2.size()) {
+                                if (PRE2 && pre2) out2[g] = *reinterpret_cast<const E2*>(&u2[PRE2 ? r : 0].t[e]);
+                                else out2[g] = ld_view_nc<E2>(in2, wb + (size_t)r * 128 + (size_t)lane * 4 + e);
+                            }
                         }
                         sbuf[pos++] = u[r].t[e];
                     }

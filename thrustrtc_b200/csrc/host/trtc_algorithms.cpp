@@ -551,7 +551,8 @@ unsigned long long run_compact(CompactSpec& c) {
     const bool vec_mode = !c.partition && c.in->elem_size() == 4 && c.in->contiguous_data() && !c.written.empty() &&
                           c.written[0]->contiguous_data() &&
                           ((!c.two && (c.mode == CM_PRED || c.mode == CM_NOT_EQUAL || c.mode == CM_NOT_PRED)) || neigh);
-    const int items2 = vec_mode ? 32 : TRTC_COMPACT2_GENERIC_ITEMS;
+    // (two-array vector forms hold their second array's rows in registers too: 16 items)
+    const int items2 = vec_mode ? (c.two ? 16 : 32) : TRTC_COMPACT2_GENERIC_ITEMS;
     const size_t tile = 256 * (two_phase ? (size_t)items2 : 16);
     const size_t tiles = (n + tile - 1) / tile;
     ViewBuf st;
