@@ -334,6 +334,11 @@ TRTC_FORCEINLINE void bulk_load_g2s(void* sdst, const void* gsrc, uint32_t bytes
                  "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+// L2 prefetch of a global range by the tensor memory accelerator (no shared memory, no
+// load/store-pipe work); address 16-byte aligned, size a multiple of 16
+TRTC_FORCEINLINE void bulk_prefetch_l2(const void* g, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(g), "r"(bytes) : "memory");
+}
 TRTC_FORCEINLINE bool mbar_try_wait(unsigned long long* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -442,7 +447,8 @@ constexpr bool radix_vbulk() {
 //      digit's run.
 template <class K, class V, bool HAS_VALS, bool DESC, int BLOCK, int ITEMS, class ST>
 __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kernel(SortBufs bufs, size_t n, SortCtrl* ctrl, int pass,
-                                                           ST* status0, ST* status1, int vals_from_index) {
+                                                           ST* status0, ST* status1, int vals_from_index,
+                                                           uint32_t pf_tiles) {
     static_assert(BLOCK == 256, "one thread per digit");
     constexpr int TILE = BLOCK * ITEMS;
     constexpr int WARPS = BLOCK / 32;
@@ -502,6 +508,21 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
     const KB* __restrict__ wk = src_k + wbase;
     const bool full = tile_base + TILE <= n;
     const uint32_t tile_n = full ? (uint32_t)TILE : (uint32_t)(n - tile_base);
+    // tiles are claimed in order, so the tile pf_tiles ahead (a fraction of the ~4 tiles per
+    // SM in flight) starts a few tile durations later: one TMA bulk prefetch brings its keys
+    // and payloads into L2 now, and its CTA's loads then wait on L2 instead of HBM (whole
+    // tiles inside [0, n) only; the prefetch is a hint and changes no result)
+    if (pf_tiles && threadIdx.x == 32) {
+        const size_t fb = tile_base + (size_t)pf_tiles * TILE;
+        if (fb + TILE <= n) {
+            const KB* fk = src_k + fb;
+            if ((reinterpret_cast<uintptr_t>(fk) & 15u) == 0) bulk_prefetch_l2(fk, (uint32_t)(TILE * sizeof(KB)));
+            if (HAS_VALS && !index_payload) {
+                const V* fv = src_v + fb;
+                if ((reinterpret_cast<uintptr_t>(fv) & 15u) == 0) bulk_prefetch_l2(fv, (uint32_t)(TILE * sizeof(V)));
+            }
+        }
+    }
     // uniform over the CTA: full tile, loaded payloads, 16-byte aligned source
     const bool vbulk = VB && full && !index_payload && ((reinterpret_cast<uintptr_t>(src_v + tile_base) & 15u) == 0);
     if (vbulk && threadIdx.x == 0) {
