@@ -15,6 +15,8 @@ struct LookbackState {
     unsigned int epoch8;            // per-launch epoch * 8: stale flags never look valid
     unsigned int* err;              // host-visible error word
     void* result;                   // optional: the last tile stores the grand total here
+    unsigned int pf_ahead = 0;      // persistent tile kernels: when a CTA claims tile t, it
+                                    // prefetches tile t + pf_ahead into L2 (0: none)
 };
 
 }  // namespace trtc

@@ -257,6 +257,9 @@ __global__ void __launch_bounds__(BLOCK, TRTC_COMPACT2_MINB) compact2_kernel(InV
             const unsigned long long t = atomicAdd(st.tile_ctr, 1ull);
             if (t == (unsigned long long)tiles + gridDim.x - 1) atomicExch(st.tile_ctr, 0ull);
             s_ticket = t;
+            // the input's tile ahead into L2 (the second array is read at selected elements only)
+            if constexpr (ViewTraits<InV>::contiguous)
+                if (st.pf_ahead) prefetch_l2_range(in._data, (size_t)(t + st.pf_ahead) * TILE, (size_t)TILE, n);
         }
         __syncthreads();
         return (size_t)s_ticket;

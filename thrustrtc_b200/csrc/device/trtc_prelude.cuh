@@ -109,6 +109,19 @@ TRTC_FORCEINLINE void backoff(uint32_t spins) {
 // One poll of a bounded wait.  Returns false when the wait must be abandoned: the poll
 // budget is spent, or another thread has already reported an error (then every waiter
 // gives up quickly instead of each spending its own budget).
+// L2 prefetch of elements [first, first + count) of a contiguous array by the tensor memory
+// accelerator (cp.async.bulk.prefetch, no multicast: no shared memory, no load/store-pipe
+// work), issued only when the whole range lies inside [0, n), starts 16-byte aligned and
+// spans a multiple of 16 bytes.  A hint: it changes no result.
+template <class E>
+TRTC_FORCEINLINE void prefetch_l2_range(const E* base, size_t first, size_t count, size_t n) {
+    if (!base || count == 0 || first + count > n) return;
+    const E* p = base + first;
+    const size_t bytes = count * sizeof(E);
+    if ((reinterpret_cast<size_t>(p) & 15u) != 0 || (bytes & 15u) != 0 || bytes >= (1u << 30)) return;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"((uint32_t)bytes) : "memory");
+}
+
 TRTC_FORCEINLINE bool spin_continue(uint32_t& spins, const uint32_t* err) {
     ++spins;
     if (spins > TRTC_SPIN_LIMIT) return false;

@@ -453,6 +453,7 @@ __global__ void __launch_bounds__(BLOCK) scan2_kernel(const T* __restrict__ in, 
             const unsigned long long t = atomicAdd(st.tile_ctr, 1ull);
             if (t == (unsigned long long)tiles + gridDim.x - 1) atomicExch(st.tile_ctr, 0ull);
             s_ticket = t;
+            if (st.pf_ahead) prefetch_l2_range(in, (size_t)(t + st.pf_ahead) * TILE, (size_t)TILE, n);
         }
         __syncthreads();
         return (size_t)s_ticket;
@@ -927,6 +928,10 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB(sizeof(T))) sbk2_kernel(
             const unsigned long long t = atomicAdd(st.tile_ctr, 1ull);
             if (t == (unsigned long long)tiles + gridDim.x - 1) atomicExch(st.tile_ctr, 0ull);
             s_ticket = t;
+            if (st.pf_ahead) {
+                prefetch_l2_range(keys, (size_t)(t + st.pf_ahead) * TILE, (size_t)TILE, n);
+                prefetch_l2_range(vals, (size_t)(t + st.pf_ahead) * TILE, (size_t)TILE, n);
+            }
         }
         __syncthreads();
         return (size_t)s_ticket;

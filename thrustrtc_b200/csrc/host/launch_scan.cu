@@ -50,6 +50,7 @@ static bool scan_t(const T* in, T* out, size_t n, const T* init, cudaStream_t s)
             return false;
         size_t grid = (size_t)(per_sm > 0 ? per_sm : 1) * sm_count();
         if (grid > tiles) grid = tiles;
+        st.pf_ahead = tile_prefetch_ahead(grid);
         ktimer_mark("", s);
         kernel<<<(unsigned)grid, SCAN_BLOCK, 0, s>>>(in, out, n, tiles, Op(), ini, st);
         count_launch();
@@ -191,6 +192,7 @@ static bool sbk_t(const K* keys, const T* vals, T* out, size_t n, const T* init,
                 return false;
             size_t grid = (size_t)(per_sm > 0 ? per_sm : 1) * sm_count();
             if (grid > tiles) grid = tiles;
+            st.pf_ahead = tile_prefetch_ahead(grid);
             ktimer_mark("", s);
             kernel<<<(unsigned)grid, SCAN_BLOCK, 0, s>>>(keys, vals, out, n, tiles, init ? *init : T(), st);
             count_launch();
@@ -298,6 +300,7 @@ static bool compact_t(const T* in, T* out, size_t n, const T* value, cudaStream_
             return false;
         size_t grid = (size_t)(per_sm > 0 ? per_sm : 1) * sm_count();
         if (grid > tiles) grid = tiles;
+        st.pf_ahead = tile_prefetch_ahead(grid);
         kernel<<<(unsigned)grid, SCAN_BLOCK, 0, s>>>(iv, Nothing(), EqualTo(), value ? *value : T(), ov, Nothing(),
                                                       Nothing(), Nothing(), n, tiles, st);
     } else {

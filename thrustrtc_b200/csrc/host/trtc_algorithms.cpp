@@ -573,6 +573,8 @@ unsigned long long run_compact(CompactSpec& c) {
         const size_t g = (size_t)sm_count() * 4;
         grid = (unsigned)(g < tiles ? g : tiles);
         params.push_back(pod_bytes<size_t>(tiles));
+        lst.pf_ahead = tile_prefetch_ahead(grid);
+        st = pod_bytes(lst);
     }
     params.push_back(st);
     if (!jit_run({"trtc_compact.cuh"}, k, grid, 256, params)) return kFail;

@@ -255,6 +255,14 @@ void* sort_ctrl_ws(cudaStream_t s, size_t bytes) {
     return w->sort_ctrl;
 }
 
+unsigned tile_prefetch_ahead(size_t grid) {
+    static const bool on = [] {
+        const char* e = getenv("TRTC_TILE_PREFETCH");
+        return !(e && std::string(e) == "0");
+    }();
+    return on ? (unsigned)grid : 0u;
+}
+
 // ---------------------------------------------------------------- allocation cap
 static std::atomic<unsigned long long> g_alloc_limit{0};
 void set_alloc_limit(unsigned long long bytes) { g_alloc_limit.store(bytes, std::memory_order_relaxed); }
