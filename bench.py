@@ -51,7 +51,7 @@ L2_BYTES = 126 * 1024 * 1024
 # scaled by the units processed (traffic grows in proportion).  Source summaries:
 # profiles/<kernel>_<workload>.md
 NCU_TRAFFIC_PER_UNIT = {
-    "sort_by_key_u32": 14.87,   # radix_pass_kernel, 2^25 pairs: (269.7 + 229.3) MB / 2^25
+    "sort_by_key_u32": 15.02,   # radix_pass_kernel, 2^25 pairs: (269.9 + 234.2) MB / 2^25
     "inclusive_scan_i32": 7.15,  # scan2_kernel, 2^26 elements: (270.8 + 208.7) MB / 2^26
     "reduce_f32": 4.07,          # reduce_kernel, 2^26 elements: (268.5 + 4.9) MB / 2^26
 }
