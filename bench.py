@@ -52,7 +52,7 @@ L2_BYTES = 126 * 1024 * 1024
 # profiles/<kernel>_<workload>.md
 NCU_TRAFFIC_PER_UNIT = {
     "sort_by_key_u32": 15.02,   # radix_pass_kernel, 2^25 pairs: (269.9 + 234.2) MB / 2^25
-    "inclusive_scan_i32": 7.15,  # scan2_kernel, 2^26 elements: (270.8 + 208.7) MB / 2^26
+    "inclusive_scan_i32": 7.31,  # scan2_kernel, 2^26 elements: (282.8 + 207.9) MB / 2^26
     "reduce_f32": 4.07,          # reduce_kernel, 2^26 elements: (268.5 + 4.9) MB / 2^26
 }
 

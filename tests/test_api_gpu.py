@@ -353,6 +353,39 @@ def test_vectorised_searches_large_and_comparator(trtc):
     assert trtc.Lower_Bound(dd, trtc.DVInt64(int(q[0])), trtc.Greater()) == int(exp[0])
 
 
+@pytest.mark.parametrize("dtype,tname", [(np.int32, "int32_t"), (np.float32, "float"), (np.uint64, "uint64_t")])
+def test_vectorised_searches_sample_edges(trtc, dtype, tname):
+    # vectorised searches against numpy's searchsorted / isin: sizes around 2^13 and up to
+    # 2^20 + 5, duplicate runs (1, 37 and 5000 equal keys), queries below the first and above
+    # the last element, ascending (Less) and descending (Greater) views
+    rng = np.random.default_rng(8)
+    for n in [8191, 8192, 8193, 100003, (1 << 20) + 5]:
+        for run in (1, 37, 5000):
+            a = np.sort((np.arange(n) // run * 3 + rng.integers(0, 2, n)).astype(dtype))
+            lo, hi = a[0], a[-1]
+            q = np.concatenate([a[rng.integers(0, n, 3000)], rng.integers(int(lo) - 5 if lo > 5 else 0,
+                                int(hi) + 6, 3000).astype(dtype),
+                                np.array([lo, hi], dtype=dtype)])
+            if dtype != np.uint64 or lo > 0:
+                q = np.concatenate([q, np.array([lo - 1], dtype=dtype)])
+            q = q.astype(dtype)
+            da, dq = trtc.device_vector_from_numpy(a), trtc.device_vector_from_numpy(q)
+            out = trtc.device_vector("uint64_t", len(q))
+            trtc.Lower_Bound_V(da, dq, out)
+            assert np.array_equal(out.to_host(), np.searchsorted(a, q, "left").astype(np.uint64)), (n, run)
+            trtc.Upper_Bound_V(da, dq, out)
+            assert np.array_equal(out.to_host(), np.searchsorted(a, q, "right").astype(np.uint64)), (n, run)
+            found = trtc.device_vector("bool", len(q))
+            trtc.Binary_Search_V(da, dq, found)
+            assert np.array_equal(found.to_host().astype(bool), np.isin(q, a)), (n, run)
+            d = a[::-1].copy()
+            dd = trtc.device_vector_from_numpy(d)
+            trtc.Lower_Bound_V(dd, dq, out, trtc.Greater())
+            assert np.array_equal(out.to_host(), (n - np.searchsorted(a, q, "right")).astype(np.uint64)), (n, run)
+            trtc.Upper_Bound_V(dd, dq, out, trtc.Greater())
+            assert np.array_equal(out.to_host(), (n - np.searchsorted(a, q, "left")).astype(np.uint64)), (n, run)
+
+
 def test_reference_zipped_program(trtc):
     # python/test/test_zipped.py with its outputs checked
     d_int_in = trtc.device_vector_from_list([0, 1, 2, 3, 4], "int32_t")
