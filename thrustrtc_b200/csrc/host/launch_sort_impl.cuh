@@ -120,7 +120,7 @@ static bool radix_sort_run(K* keys, V* vals0, size_t n, cudaStream_t s, int vals
         // L2 prefetch distance of the pass kernel: 1.5 tiles per SM ahead (B200, 2^28 u32 pairs:
         // 5.739 ms without, 5.585 ms at 222 tiles, within 0.2 % from 148 to 444 tiles, slower
         // again past one wave of resident CTAs as the prefetched tiles crowd L2)
-        const uint32_t pf = (uint32_t)(sms * 3 / 2);
+        const uint32_t pf = tile_prefetch_ahead((size_t)sms * 3 / 2);
         for (int p = 0; p < D; p++) {
             pass_kernel<<<(unsigned)tiles, BLOCK, smem, s>>>(bufs, n, ctrl, p, (ST*)st0, (ST*)st1, vals_from_index, pf);
             ktimer_mark("radix_pass_kernel", s);

@@ -255,12 +255,12 @@ void* sort_ctrl_ws(cudaStream_t s, size_t bytes) {
     return w->sort_ctrl;
 }
 
-unsigned tile_prefetch_ahead(size_t grid) {
+unsigned tile_prefetch_ahead(size_t tiles) {
     static const bool on = [] {
         const char* e = getenv("TRTC_TILE_PREFETCH");
         return !(e && std::string(e) == "0");
     }();
-    return on ? (unsigned)grid : 0u;
+    return on ? (unsigned)tiles : 0u;
 }
 
 // ---------------------------------------------------------------- allocation cap
