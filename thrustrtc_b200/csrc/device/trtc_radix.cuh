@@ -380,10 +380,14 @@ template <bool B> struct BoolC { static constexpr bool value = B; };
 // pipes: items i with i % MIXP < MIXB use eight bit ballots (ALU and vote instructions),
 // the others atomicOr their lane bit into a per-warp mask per digit in shared memory (LSU).
 // Measured on B200 (2^28 u32 pairs): masks alone move the pass onto the LSU pipe, ballots
-// alone onto issue; one item in three on ballots balances them.  __match_any_sync was 50 %
-// slower than either.
+// alone onto issue; one item in three on ballots balances them for pairs, one in five for
+// keys alone (no payload traffic on the LSU pipe; 2^28 u32 keys 4.605 -> 4.569 ms, pairs
+// 5.701 -> 5.727 ms at one in five).  __match_any_sync was 50 % slower than either.
 #ifndef TRTC_RADIX_MIXP
 #define TRTC_RADIX_MIXP 3
+#endif
+#ifndef TRTC_RADIX_MIXP_KEYS
+#define TRTC_RADIX_MIXP_KEYS 5
 #endif
 #ifndef TRTC_RADIX_MIXB
 #define TRTC_RADIX_MIXB 1
@@ -452,6 +456,9 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
     static_assert(BLOCK == 256, "one thread per digit");
     constexpr int TILE = BLOCK * ITEMS;
     constexpr int WARPS = BLOCK / 32;
+    constexpr int MIXP = HAS_VALS ? TRTC_RADIX_MIXP : TRTC_RADIX_MIXP_KEYS;
+    static_assert(TRTC_RADIX_MIXB < TRTC_RADIX_MIXP_KEYS || TRTC_RADIX_MIXB >= TRTC_RADIX_MIXP,
+                  "keys-only and pair sorts agree on whether digit masks are used");
     constexpr bool FLOATKEY = is_same<K, float>::value || is_same<K, double>::value;
     typedef StatusBits<ST> SB;
     typedef typename RadixKey<K>::B KB;
@@ -553,7 +560,7 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t d = radix_digit_sel<K, DESC>(keys[i], sel, hi);
             uint32_t peers;
-            if ((i % TRTC_RADIX_MIXP) < TRTC_RADIX_MIXB) {
+            if ((i % MIXP) < TRTC_RADIX_MIXB) {
                 peers = FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, (uint32_t)i * 32u + lane < warp_n);
 #pragma unroll
                 for (int b = 0; b < 8; b++) {
@@ -565,9 +572,8 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
                 const bool valid = FULL || (uint32_t)i * 32u + lane < warp_n;
                 // the two mask sets alternate over the mask-ranked items, so a set is reused
                 // only after the other set's item and its two warp barriers
-                const int ors_before = i - ((i / TRTC_RADIX_MIXP) * TRTC_RADIX_MIXB +
-                                            ((i % TRTC_RADIX_MIXP) < TRTC_RADIX_MIXB ? (i % TRTC_RADIX_MIXP)
-                                                                                     : TRTC_RADIX_MIXB));
+                const int ors_before = i - ((i / MIXP) * TRTC_RADIX_MIXB +
+                                            ((i % MIXP) < TRTC_RADIX_MIXB ? (i % MIXP) : TRTC_RADIX_MIXB));
                 uint32_t* wm = s_wmatch + warp * 512 + (ors_before & 1) * 256;
                 if (valid) atomicOr(&wm[d], 1u << lane);
                 __syncwarp();
