@@ -1282,7 +1282,7 @@ __global__ void __launch_bounds__(BLOCK, TRTC_SBK2_MINB(sizeof(T))) sbk2_kernel(
 template <class E, class T, class Op, class UOp, bool HAS_UOP, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) reduce_kernel(const E* __restrict__ in, size_t n, Op op, UOp uop, T* partials,
                                                        int* partial_has, uint32_t* done_ctr, T* result, int has_init,
-                                                       T init, uint32_t prefetch = 0) {
+                                                       T init) {
     constexpr int VEC = VecWidth<E>::V;
     constexpr int WARPS = BLOCK / 32;
     __shared__ T s_w[WARPS];
@@ -1307,13 +1307,6 @@ __global__ void __launch_bounds__(BLOCK) reduce_kernel(const E* __restrict__ in,
         // U independent 16-byte loads in flight per thread
         constexpr int U = 4;
         for (vi += gsz; vi + (U - 1) * gsz < nvec; vi += U * gsz) {
-            // the CTA's rows of the next round into L2 (one bulk prefetch per row; B200, 2^28
-            // f32: 0.2096 -> 0.2003 ms on one box; the same in the sort's histogram kernel,
-            // whose loop has this shape, measured 2 % slower and is not done there)
-            if (prefetch && threadIdx.x == 0)
-#pragma unroll
-                for (int r = 0; r < U; r++)
-                    prefetch_l2_range(reinterpret_cast<const uint4*>(in), vi + (size_t)(U + r) * gsz, (size_t)BLOCK, nvec);
             union { uint4 q; E e[VEC]; } w[U];
 #pragma unroll
             for (int r = 0; r < U; r++) w[r].q = reinterpret_cast<const uint4*>(in)[vi + r * gsz];

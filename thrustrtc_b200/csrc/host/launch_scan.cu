@@ -120,7 +120,7 @@ static bool reduce_t(const T* in, size_t n, const T* init, void** result_dev, cu
     ktimer_mark("", s);
     reduce_kernel<T, T, Op, Identity, false, BLOCK><<<(unsigned)grid, BLOCK, 0, s>>>(
         in, n, Op(), Identity(), (T*)w->partials, w->partial_has, w->done_ctr, (T*)w->result, init ? 1 : 0,
-        init ? *init : T(), tile_prefetch_ahead(1));
+        init ? *init : T());
     count_launch();
     ktimer_mark("reduce_kernel", s);
     *result_dev = w->result;
