@@ -334,11 +334,6 @@ TRTC_FORCEINLINE void bulk_load_g2s(void* sdst, const void* gsrc, uint32_t bytes
                  "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
-// L2 prefetch of a global range by the tensor memory accelerator (no shared memory, no
-// load/store-pipe work); address 16-byte aligned, size a multiple of 16
-TRTC_FORCEINLINE void bulk_prefetch_l2(const void* g, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(g), "r"(bytes) : "memory");
-}
 TRTC_FORCEINLINE bool mbar_try_wait(unsigned long long* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -521,14 +516,8 @@ __global__ void __launch_bounds__(BLOCK, TRTC_RADIX_MINB(ITEMS)) radix_pass_kern
     // tiles inside [0, n) only; the prefetch is a hint and changes no result)
     if (pf_tiles && threadIdx.x == 32) {
         const size_t fb = tile_base + (size_t)pf_tiles * TILE;
-        if (fb + TILE <= n) {
-            const KB* fk = src_k + fb;
-            if ((reinterpret_cast<uintptr_t>(fk) & 15u) == 0) bulk_prefetch_l2(fk, (uint32_t)(TILE * sizeof(KB)));
-            if (HAS_VALS && !index_payload) {
-                const V* fv = src_v + fb;
-                if ((reinterpret_cast<uintptr_t>(fv) & 15u) == 0) bulk_prefetch_l2(fv, (uint32_t)(TILE * sizeof(V)));
-            }
-        }
+        prefetch_l2_range(src_k, fb, (size_t)TILE, n);
+        if (HAS_VALS && !index_payload) prefetch_l2_range(src_v, fb, (size_t)TILE, n);
     }
     // uniform over the CTA: full tile, loaded payloads, 16-byte aligned source
     const bool vbulk = VB && full && !index_payload && ((reinterpret_cast<uintptr_t>(src_v + tile_base) & 15u) == 0);
