@@ -69,8 +69,8 @@ void* sort_ctrl_ws(cudaStream_t s, size_t bytes);
 // fails like an out-of-memory one, before anything is launched
 void set_alloc_limit(unsigned long long bytes);
 // L2 prefetch distance, in tiles, of the kernels that claim tiles in order: `tiles` (the
-// persistent kernels pass their grid, one tile per CTA ahead; the sort's digit pass 1.5 tiles
-// per SM), or 0 when TRTC_TILE_PREFETCH=0 is set in the environment
+// persistent kernels pass half their grid; the sort's digit pass 1.5 tiles per SM), or 0 when
+// TRTC_TILE_PREFETCH=0 is set in the environment
 unsigned tile_prefetch_ahead(size_t tiles);
 // stream-ordered temporaries (cached by the CUDA memory pool)
 void* tmp_alloc(size_t bytes, cudaStream_t s);
