@@ -573,7 +573,7 @@ unsigned long long run_compact(CompactSpec& c) {
         const size_t g = (size_t)sm_count() * 4;
         grid = (unsigned)(g < tiles ? g : tiles);
         params.push_back(pod_bytes<size_t>(tiles));
-        lst.pf_ahead = tile_prefetch_ahead(grid);
+        lst.pf_ahead = tile_prefetch_ahead(grid / 2);  // half a grid ahead, as the built-in launches
         st = pod_bytes(lst);
     }
     params.push_back(st);
